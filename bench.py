@@ -1,0 +1,371 @@
+"""Benchmark: GRE superstep suite on a seeded RMAT graph, one JSON line.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--scale S]
+
+Workload (ours, per GPU): RMAT scale 26, edge factor 16, symmetrised and de-duplicated
+(a/b/c = 0.57/0.19/0.19, seeded), uint32 ids, uint64 offsets, SSSP weights uint32 in
+[1, 255]; generated on the device.  One step = the plain suite of the reference's plugins:
+PageRank 20 supersteps (FP64, power iteration), direction-optimising BFS from one source,
+SSSP from one source, connected components, and betweenness from 64 sources in one batched
+pass.  Sources are seeded samples of non-isolated vertices, different every step.
+
+Metric: GTEPS = traversed edges / device time, summed over the suite (PageRank: arcs x
+supersteps; BFS/SSSP: undirected edges of the reached component (Graph500); CC: undirected
+edges; BC: sources x undirected edges).  Per-algorithm GTEPS and algorithmic HBM GB/s are
+reported beside it.  `value` uses device-resident outputs; `e2e` runs the same calls with
+pinned host outputs, the device->host copies inside the timed region.
+
+--impl reference runs the reference GRE engine (compiled from its headers into oracle/_ref/)
+on the host CPU over a bounded sample (RMAT scale 16, same suite) and prints the same line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GTEPS & HBM GB/s at RMAT-26 on 1 B200; batched/adjoint vs plain at equal results"
+SEED = 26
+WSEED = 20240601
+PR_ITERS = 20
+BC_SOURCES = 64
+CPU_SCALE = 16
+CPU_BC_SOURCES = 8  # betweenness sources per step in the bounded CPU sample
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+# ----------------------------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ----------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for i, nm in enumerate(names):
+                if parts[5 + i].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per PageRank superstep from the committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", "pagerank_pull_superstep.md")
+    try:
+        for line in open(p):
+            m = re.match(r"\s*traffic_bytes_per_superstep_s26:\s*([0-9.eE+]+)", line)
+            if m:
+                return float(m.group(1))
+    except OSError:
+        pass
+    return None
+
+
+# ----------------------------------------------------------------------------------------------
+# reference arm / CPU baseline: the reference engine on the host
+# ----------------------------------------------------------------------------------------------
+def reference_suite(scale: int, reps: int, workdir: str):
+    """Runs the reference suite `reps` times on RMAT-`scale`; returns per-rep (edges, seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import graphine_b200.gre as G
+    import oracle as O
+
+    n, off, col = G.rmat_host(scale, 16, SEED, True)
+    prefix = os.path.join(workdir, f"rmat{scale}")
+    G.write_edgelists(prefix, n, off, col, 4)
+    roots = G.sample_sources(off, reps * CPU_BC_SOURCES, 5)
+    G.write_roots(prefix, roots)
+    R = O.Restatement.from_csr(n, off, col)
+    m_arcs = len(col)
+    m_und = m_arcs // 2
+    # reached-component edge counts (Graph500 numerator) from the oracle's levels
+    deg = np.diff(off.astype(np.int64))
+    lv = R.bfs_many(roots)
+    comp_edges = [int(deg[lv[i] >= 0].sum() // 2) for i in range(len(roots))]
+    t = {}
+    _, run = O.run_reference("pagerank", prefix, "iter", PR_ITERS, reps)
+    t["pagerank"] = run.seconds
+    _, run = O.run_reference("bfs", prefix, reps)  # the first `reps` roots
+    t["bfs"] = run.seconds[0::2]  # runs alternate: BFS plugin, Forward levels
+    _, run = O.run_reference("sssp", prefix, WSEED, reps)
+    t["sssp"] = run.seconds
+    _, run = O.run_reference("cc", prefix, reps)
+    t["cc"] = run.seconds
+    _, run = O.run_reference("bc", prefix, reps * CPU_BC_SOURCES)
+    t["bc"] = [sum(run.seconds[r * CPU_BC_SOURCES:(r + 1) * CPU_BC_SOURCES]) for r in range(reps)]
+    out = []
+    for r in range(reps):
+        edges = m_arcs * PR_ITERS + comp_edges[r] + comp_edges[r] + m_und + CPU_BC_SOURCES * m_und
+        secs = t["pagerank"][r] + t["bfs"][r] + t["sssp"][r] + t["cc"][r] + t["bc"][r]
+        out.append((edges, secs))
+    return out, {"n": n, "m": m_arcs}
+
+
+def cpu_cores_used():
+    return 12  # the reference engine's fixed worker pool (Engine.hpp:211); plus its master thread
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    with tempfile.TemporaryDirectory() as td:
+        res, info = reference_suite(CPU_SCALE, args.warmup + args.steps, td)
+    timed = res[args.warmup:]
+    edges = sum(e for e, _ in timed)
+    secs = sum(s for _, s in timed)
+    value = edges / secs / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+u32", "data": "synthetic",
+        "config": {"workload": f"GRE suite (PageRank-20 iter, BFS, SSSP, CC, BC {CPU_BC_SOURCES} src) on RMAT scale {CPU_SCALE} "
+                               f"symmetric EF16 (bounded sample of the scale-26 workload)",
+                   "graph_n": info["n"], "graph_arcs": info["m"], "parallelism": "cpu"},
+        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": cpu_cores_used(), "kind": "reference",
+                         "sample": f"RMAT-{CPU_SCALE} symmetric, reference GRE engine -O0 np=1, "
+                                   f"engine.run timed (MPI_Wtime), {args.steps} suites"},
+        "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------------------------
+# our arm
+# ----------------------------------------------------------------------------------------------
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import graphine_b200.gre as G
+
+    dist = world > 1
+    if dist:
+        import torch.distributed as tdist
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+
+    g = G.Graph.rmat(args.scale, 16, SEED, True, device=local_rank)
+    g.set_weights_hash(WSEED)
+    n, m = g.n, g.m
+    outdeg = g.getOutdegree()
+    nz = np.flatnonzero(outdeg > 0)
+    rng = np.random.default_rng(1000 + rank)
+    nsteps = args.warmup + args.steps
+    one_src = rng.choice(nz, size=nsteps, replace=False).astype(np.uint32)
+    bc_src = [np.sort(rng.choice(nz, size=args.bc_sources, replace=False)).astype(np.uint32) for _ in range(nsteps)]
+
+    # device outputs (value)
+    pr_d = torch.empty(n, dtype=torch.float64, device=dev)
+    lv_d = torch.empty(n, dtype=torch.int32, device=dev)
+    ds_d = torch.empty(n, dtype=torch.int32, device=dev)  # uint32 payload
+    cc_d = torch.empty(n, dtype=torch.int32, device=dev)
+    bc_d = torch.empty(n, dtype=torch.float64, device=dev)
+    names = ["pagerank", "bfs", "sssp", "cc", "bc64"]
+
+    def suite(i, outs, bcs=None):
+        pr_o, lv_o, ds_o, cc_o, bc_o = outs
+        r = []
+        _, s = G.pagerank(g, G.PR_ITER, 0.85, PR_ITERS, out=pr_o)
+        r.append(s)
+        _, s = G.bfs(g, one_src[i:i + 1], out=lv_o)
+        r.append(s)
+        _, s = G.sssp(g, one_src[i:i + 1], out=ds_o)
+        r.append(s)
+        _, s = G.cc(g, out=cc_o)
+        r.append(s)
+        _, s = G.bc(g, bc_src[i] if bcs is None else bcs, batched=True, out=bc_o)
+        r.append(s)
+        return r
+
+    dev_outs = (pr_d, lv_d, ds_d, cc_d, bc_d)
+    for i in range(args.warmup):
+        suite(i, dev_outs)
+    torch.cuda.synchronize()
+    if dist:
+        tdist.barrier()
+    torch.cuda.synchronize()
+    l0 = G.launch_count()
+    per = {k: {"ms": 0.0, "edges": 0, "bytes": 0, "arcs": 0} for k in names}
+    with ClockSampler(local_rank) as clk:
+        for i in range(args.warmup, nsteps):
+            for k, s in zip(names, suite(i, dev_outs)):
+                per[k]["ms"] += s.device_ms
+                per[k]["edges"] += s.traversed_edges
+                per[k]["bytes"] += s.algo_bytes
+                per[k]["arcs"] += s.arcs_traversed
+        torch.cuda.synchronize()
+    launches = G.launch_count() - l0
+    if dist:
+        tdist.barrier()
+    torch.cuda.synchronize()
+    tot_ms = sum(v["ms"] for v in per.values())
+    tot_edges = sum(v["edges"] for v in per.values())
+
+    # e2e: same calls, pinned host outputs (device->host copies inside each call's timed span)
+    pin = lambda dt, k: torch.empty(k, dtype=dt, pin_memory=True).numpy()  # noqa: E731
+    host_outs = (pin(torch.float64, n), pin(torch.int32, n), pin(torch.int32, n), pin(torch.int32, n),
+                 pin(torch.float64, n))
+    src_pinned = pin(torch.int32, args.bc_sources).view(np.uint32)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_edges = 0
+    for i in range(args.warmup, nsteps):
+        src_pinned[:] = bc_src[i]
+        res = suite(i, host_outs, src_pinned)
+        e2e_edges += sum(s.traversed_edges for s in res)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+
+    # max over ranks of the time, sum of the work
+    if dist:
+        t = torch.tensor([tot_ms, e2e_s], dtype=torch.float64, device=dev)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        w = torch.tensor([float(tot_edges), float(e2e_edges)], dtype=torch.float64, device=dev)
+        tdist.all_reduce(w, op=tdist.ReduceOp.SUM)
+        max_ms, max_e2e = float(t[0]), float(t[1])
+        all_edges, all_e2e_edges = float(w[0]), float(w[1])
+    else:
+        max_ms, max_e2e, all_edges, all_e2e_edges = tot_ms, e2e_s, float(tot_edges), float(e2e_edges)
+    if rank != 0:
+        return 0
+
+    value = all_edges / (max_ms * 1e-3) / 1e9
+    e2e_value = all_e2e_edges / max_e2e / 1e9
+    peak, peak_kind = measured_peak()
+    pr = per["pagerank"]
+    pr_iter_ms = pr["ms"] / (args.steps * PR_ITERS)
+    pr_bytes_iter = 8 * (n + 1) + 12 * m + 20 * n
+    achieved = pr_bytes_iter / (pr_iter_ms * 1e-3) / 1e9
+    per_alg = {}
+    for k, v in per.items():
+        per_alg[k] = {"ms_per_step": v["ms"] / args.steps, "gteps": v["edges"] / (v["ms"] * 1e-3) / 1e9 if v["ms"] else None,
+                      "hbm_gbs_algorithmic": v["bytes"] / (v["ms"] * 1e-3) / 1e9 if v["ms"] else None,
+                      "share": v["ms"] / tot_ms}
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        with tempfile.TemporaryDirectory() as td:
+            res, info = reference_suite(CPU_SCALE, 1, td)
+        e, s = res[0]
+        cpu = {"value": e / s / 1e9, "unit": "GTEPS", "cores": cpu_cores_used(), "kind": "reference",
+               "sample": f"one suite on RMAT-{CPU_SCALE} symmetric (n={info['n']}, arcs={info['m']}), reference GRE "
+                         f"engine -O0 np=1, engine.run timed; BC from {CPU_BC_SOURCES} sources"}
+    d2h = n * (8 + 4 + 4 + 4 + 8)
+    line = {
+        "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64+u32", "data": "synthetic",
+        "config": {"workload": f"GRE suite on RMAT scale {args.scale} EF16 symmetric: PageRank-{PR_ITERS} (power "
+                               f"iteration), DO-BFS 1 src, SSSP 1 src (u32 w in [1,255]), CC, BC {args.bc_sources} src "
+                               f"batched", "graph_n": n, "graph_arcs": m, "parallelism": f"replica x{world}",
+                   "l2": "inputs larger than L2 (graph > 126 MB)"},
+        "per_algorithm": per_alg,
+        "roofline": {"bound": "hbm", "kernel": "PageRank pull superstep (degree-binned row kernels)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "bytes_per_launch": pr_bytes_iter,
+                     "traffic": profiled_traffic()},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": 4 * (1 + 1 + args.bc_sources),
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=int, default=26)
+    ap.add_argument("--bc-sources", type=int, default=BC_SOURCES)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local_rank = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as tdist
+
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        return run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as tdist
+
+            tdist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

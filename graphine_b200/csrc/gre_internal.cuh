@@ -1,0 +1,240 @@
+// Internal definitions of libgre_gpu.so: the graph handle, per-graph scratch workspace, error
+// plumbing and small device helpers shared by the kernel translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/gre_gpu.h"
+
+namespace gre {
+
+// ---------------------------------------------------------------------------------------------
+// Errors: every ABI call returns a status; the text of the last failure is kept per thread.
+// ---------------------------------------------------------------------------------------------
+void set_error(const char* fmt, ...);
+void clear_error();
+int cuda_status(cudaError_t e, const char* what, const char* file, int line);
+
+#define GRE_CUDA(call)                                                          \
+  do {                                                                          \
+    cudaError_t gre_e_ = (call);                                                \
+    if (gre_e_ != cudaSuccess) return ::gre::cuda_status(gre_e_, #call, __FILE__, __LINE__); \
+  } while (0)
+
+#define GRE_CHECK(expr)        \
+  do {                         \
+    int gre_s_ = (expr);       \
+    if (gre_s_) return gre_s_; \
+  } while (0)
+
+#define GRE_LAUNCH_CHECK() GRE_CUDA(cudaGetLastError())
+
+// ---------------------------------------------------------------------------------------------
+// Scratch workspace: named device buffers owned by a graph handle, grown on demand and kept
+// until the handle is freed, so repeated runs do no allocation.
+// ---------------------------------------------------------------------------------------------
+enum WsSlot {
+  WS_A = 0, WS_B, WS_C, WS_D, WS_E, WS_F, WS_G, WS_H, WS_I, WS_J, WS_K, WS_L,
+  WS_COUNTERS,   // small per-run counters (device-side)
+  WS_CUB,        // CUB temporary storage
+  WS_OUTBUF,     // device staging of results bound for host memory
+  WS_OUTBUF2,
+  // betweenness state (kept apart from the slots the BFS routines use)
+  WS_BC0, WS_BC1, WS_BC2, WS_BC3, WS_BC4, WS_BC5, WS_BC6, WS_BC7,
+  WS_NSLOTS
+};
+
+struct Workspace {
+  void* ptr[WS_NSLOTS] = {};
+  size_t bytes[WS_NSLOTS] = {};
+  int get(int slot, size_t nbytes, void** out);
+  void release();
+};
+
+// Degree bins of one adjacency (rows grouped by the number of lanes that process them).
+struct DegreeBins {
+  bool ready = false;
+  static const int NB = 8;  // 1,2,4,8,16,32 lanes, CTA per row, multi-CTA per row
+  uint64_t count[NB] = {};
+  uint64_t start[NB] = {};   // offsets into `rows`
+  uint32_t* rows = nullptr;  // row ids grouped by bin (device)
+  uint64_t n_hub_chunks = 0; // chunks of the multi-CTA bin
+  uint64_t* hub_chunk_row = nullptr;   // per chunk: index into the multi-CTA bin
+  uint64_t* hub_chunk_begin = nullptr; // per chunk: first arc
+  uint64_t* hub_chunk_first = nullptr; // per multi-CTA row: first chunk id (size count+1)
+};
+
+// Rows longer than `ch` arcs split into fixed chunks of `ch` arcs from the row start.  Partial
+// sums of the chunks are added in chunk order, which fixes the association order of a row's
+// sum independently of how many threads work on it.
+struct ChunkTable {
+  bool ready = false;
+  uint64_t ch = 0;
+  uint64_t nrows = 0, nchunks = 0;
+  uint32_t* rows = nullptr;         // long rows
+  uint64_t* chunk_row = nullptr;    // chunk -> index into rows
+  uint64_t* chunk_begin = nullptr;  // chunk -> first arc
+  uint64_t* first = nullptr;        // long row i -> first chunk (nrows + 1 entries)
+};
+
+}  // namespace gre
+
+struct gre_graph_s {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  uint64_t n = 0, m = 0;
+  uint32_t flags = 0;  // gre_dir | gre_graph_flags
+  // CSR (out-arcs)
+  uint64_t* off = nullptr;
+  uint32_t* col = nullptr;
+  // CSC (in-arcs); alias the CSR when the graph is symmetric
+  uint64_t* roff = nullptr;
+  uint32_t* rcol = nullptr;
+  uint64_t* rarc = nullptr;  // CSC slot -> CSR arc id (built on demand)
+  uint32_t* outdeg = nullptr;
+  uint32_t* indeg = nullptr;  // aliases outdeg when symmetric
+  // weights
+  uint32_t* w32 = nullptr;
+  double* w64 = nullptr;
+  double* rw64 = nullptr;  // FP64 weights in CSC order (built on demand)
+  uint64_t max_outdeg = 0, max_indeg = 0;
+  gre::Workspace ws;
+  gre::DegreeBins bins_in, bins_out;
+  gre::ChunkTable bc_chunks;       // in-arc rows longer than 512 arcs (betweenness)
+  uint64_t* bc_fpool = nullptr;    // per-level frontier words of the batched betweenness
+  uint64_t bc_fpool_levels = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  bool symmetric() const { return (flags & GRE_GRAPH_SYMMETRIC) != 0; }
+};
+
+namespace gre {
+
+// ---------------------------------------------------------------------------------------------
+// Host helpers
+// ---------------------------------------------------------------------------------------------
+inline int grid_for(uint64_t work, int block, int max_blocks_per_sm = 8) {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  uint64_t b = (work + block - 1) / block;
+  uint64_t cap = (uint64_t)sms * max_blocks_per_sm;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+int num_sms();
+
+// Pointer on the device?  (cudaPointerGetAttributes: device or managed memory)
+bool is_device_ptr(const void* p);
+
+// Make the graph's device current.
+int use_graph(gre_graph g);
+
+// Input array of `count` T: device pointer returned as is, host data staged into `slot`.
+template <class T>
+int stage_input(gre_graph g, const T* p, uint64_t count, int slot, const T** dev) {
+  if (!p) {
+    *dev = nullptr;
+    return GRE_SUCCESS;
+  }
+  if (is_device_ptr(p)) {
+    *dev = p;
+    return GRE_SUCCESS;
+  }
+  void* d = nullptr;
+  GRE_CHECK(g->ws.get(slot, sizeof(T) * (count ? count : 1), &d));
+  if (count) GRE_CUDA(cudaMemcpyAsync(d, p, sizeof(T) * count, cudaMemcpyHostToDevice, g->stream));
+  *dev = (const T*)d;
+  return GRE_SUCCESS;
+}
+
+// Output array: a device pointer is written in place; a host pointer gets a device staging
+// buffer in `slot` and is filled by finish_output.
+template <class T>
+int prepare_output(gre_graph g, T* p, uint64_t count, int slot, T** dev) {
+  if (is_device_ptr(p)) {
+    *dev = p;
+    return GRE_SUCCESS;
+  }
+  void* d = nullptr;
+  GRE_CHECK(g->ws.get(slot, sizeof(T) * (count ? count : 1), &d));
+  *dev = (T*)d;
+  return GRE_SUCCESS;
+}
+
+template <class T>
+int finish_output(gre_graph g, T* p, const T* dev, uint64_t count) {
+  if ((const void*)p != (const void*)dev && count)
+    GRE_CUDA(cudaMemcpyAsync(p, dev, sizeof(T) * count, cudaMemcpyDeviceToHost, g->stream));
+  return GRE_SUCCESS;
+}
+
+// Timing of one ABI call on the graph's stream.
+struct RunTimer {
+  gre_graph g;
+  explicit RunTimer(gre_graph gg) : g(gg) { cudaEventRecord(g->ev0, g->stream); }
+  int stop(gre_stats* st) {
+    GRE_CUDA(cudaEventRecord(g->ev1, g->stream));
+    GRE_CUDA(cudaEventSynchronize(g->ev1));
+    float ms = 0;
+    GRE_CUDA(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
+    if (st) st->device_ms = ms;
+    return GRE_SUCCESS;
+  }
+};
+
+inline void stats_reset(gre_stats* st) {
+  if (!st) return;
+  st->supersteps = 0;
+  st->n_recorded = 0;
+  st->arcs_traversed = 0;
+  st->traversed_edges = 0;
+  st->algo_bytes = 0;
+  st->device_ms = 0;
+}
+inline void stats_record(gre_stats* st, uint64_t active) {
+  if (st && st->n_recorded < GRE_MAX_RECORDED_SUPERSTEPS) st->active[st->n_recorded++] = active;
+}
+
+// Degree bins of the CSC (in = true) or CSR; built once per graph.
+int ensure_bins(gre_graph g, bool in);
+// CSC slot -> CSR arc map; built once per graph.
+int ensure_rarc(gre_graph g);
+// Undirected edge count with both endpoints in a reached set (Graph500 TEPS numerator).
+int count_reached_edges(gre_graph g, const int32_t* level, uint64_t* edges);
+// Direction-optimising BFS levels from device roots (uses slots WS_A..WS_G, WS_COUNTERS, WS_CUB).
+int bfs_levels(gre_graph g, const uint32_t* droots, uint32_t nroots, int32_t* level, gre_stats* st, bool record);
+
+// ---------------------------------------------------------------------------------------------
+// Device helpers
+// ---------------------------------------------------------------------------------------------
+#ifdef __CUDACC__
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+template <class T>
+__device__ __forceinline__ T ldg_nc(const T* p) { return __ldg(p); }
+
+// Warp-aggregated append of one item per active lane into a queue.
+__device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
+  const uint32_t mask = __ballot_sync(0xffffffffu, want);
+  if (!mask) return 0xffffffffu;
+  const uint32_t lane = lane_id();
+  const uint32_t leader = __ffs(mask) - 1;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  return want ? base + __popc(mask & ((1u << lane) - 1u)) : 0xffffffffu;
+}
+#endif
+
+}  // namespace gre

@@ -1,0 +1,218 @@
+/*
+ * gre_gpu.h — C ABI of the B200-native GRE superstep engine (libgre_gpu.so).
+ *
+ * This is the drop-in boundary for the hot path of the reference GRE engine
+ * (NCIC-PARALLEL/Graphine): the vertex-centric superstep init -> scatter -> combine -> apply ->
+ * vote-to-halt of SynchronousEngine (include/Engine/Engine.hpp:180-406,437-798) for the
+ * PageRank, BFS, SSSP, ConnectedComponents and BC plugins (include/Kernels/), together
+ * with the `<prefix>.meta` + `<prefix>.edges.<i>` loader (include/Graph/GraphIngress.hpp).
+ * The reference is a header-only C++ template library with no FFI; each entry point below
+ * names the reference function or driver step whose role it takes.
+ *
+ * Conventions
+ *  - Every call returns a status code (gre_status below) and never exits the process.
+ *  - Vertex ids are uint32, arc offsets uint64 (the reference: lvid_t = uint32,
+ *    lidx_t = size_t; include/Types.hpp:13-18).
+ *  - Buffers passed in or out may live in host memory or in device memory of the graph's
+ *    device; the library checks which with cudaPointerGetAttributes and copies as needed.
+ *    Outputs are caller-allocated.  Host outputs are complete when the call returns.
+ *  - One CUDA stream per graph handle.  Calls on one handle are serialised by the caller;
+ *    distinct handles may be used from different threads.
+ *  - Symbols under "host utilities" run on the CPU only and need no GPU.
+ */
+#ifndef GRE_GPU_H
+#define GRE_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes 0..8 keep the values of enum GRE_Status (include/Status.hpp:5-14). */
+enum gre_status {
+  GRE_SUCCESS = 0,
+  GRE_FAILURE = 1,
+  GRE_NOBUFFER = 2,
+  GRE_NULL = 3,
+  GRE_FINISHED = 4,
+  GRE_UNFINISHED = 5, /* also: max supersteps reached before the frontier emptied */
+  GRE_INITIALIZED = 6,
+  GRE_UNINITIALIZED = 7,
+  GRE_NOT_IMPLEMENTED = 8,
+  GRE_INVALID_ARG = 9, /* added: bad size, vertex id out of range, missing weights ... */
+  GRE_IO_ERROR = 10,   /* added: missing/garbled .meta / .edges.<i> / .roots */
+  GRE_CUDA_ERROR = 11, /* added: a CUDA runtime call failed (see gre_last_error) */
+  GRE_OOM = 12,        /* added: device or host allocation failed */
+  GRE_TIMEOUT = 13,    /* added: a bounded device-side wait gave up */
+  GRE_NO_DEVICE = 14   /* added: no usable CUDA device */
+};
+
+/* Edge directions: enum Dir {Out, In, InOut} (include/Types.hpp:33). */
+enum gre_dir { GRE_DIR_OUT = 0, GRE_DIR_IN = 1, GRE_DIR_INOUT = 2 };
+
+/* Graph flags for the loaders (OR-ed with a direction). */
+enum gre_graph_flags {
+  GRE_GRAPH_SYMMETRIC = 0x10 /* every arc (u,v) has its reverse: the CSR doubles as CSC */
+};
+
+/* PageRank variants. */
+enum gre_pr_variant {
+  GRE_PR_REFERENCE = 0, /* Kernels/PageRank.hpp verbatim: pr_scatter never refreshed */
+  GRE_PR_ITER = 1       /* power iteration: pr_scatter = pr/outdeg refreshed in apply */
+};
+
+#define GRE_MAX_RECORDED_SUPERSTEPS 1024 /* default max_nSupersteps (Engine.hpp:108) */
+
+/* Per-run statistics.  `active` mirrors the per-superstep line the reference prints
+ * ("Superstep-k: Number of active vertices...", Engine.hpp:392-398). */
+typedef struct gre_stats {
+  uint32_t supersteps;     /* SynchronousEngine::getSuperstepCount() (Engine.hpp:1307-1309) */
+  uint32_t n_recorded;     /* valid entries of active[] */
+  uint64_t arcs_traversed; /* arcs the kernels scanned */
+  uint64_t traversed_edges;/* edges counted for TEPS (definition per algorithm) */
+  uint64_t algo_bytes;     /* algorithmic HBM bytes of the run (byte model of each kernel) */
+  double device_ms;        /* device time of the run, CUDA events on the graph's stream */
+  uint64_t active[GRE_MAX_RECORDED_SUPERSTEPS];
+} gre_stats;
+
+typedef struct gre_graph_s* gre_graph;
+
+/* ---------------------------------------------------------------------------------------
+ * Status and devices
+ * ------------------------------------------------------------------------------------- */
+/* GRE_Status_Parser::parse (include/Status.hpp:17-30), extended to the added codes. */
+const char* gre_status_str(int status);
+/* Text of the last error raised on the calling thread ("" if none). */
+const char* gre_last_error(void);
+/* Number of CUDA devices (0 on a host without GPU). */
+int gre_device_count(int* count);
+/* Kernels this library has launched so far in the process (its own and the CUB primitives
+ * compiled into it).  No reference counterpart: instrumentation for benchmarks. */
+uint64_t gre_launch_count(void);
+
+/* ---------------------------------------------------------------------------------------
+ * Graph: device CSR (out-arcs) and CSC (in-arcs), uint32 ids, uint64 offsets.
+ * Replaces DistributedGraph<GraphInCSR> at one rank (Graph/DistributedGraph.hpp:23-273,
+ * Graph/LocalGraph.hpp:23-200).
+ * ------------------------------------------------------------------------------------- */
+/* DistributedGraph::ingress<dir>(comm, pool, prefix, "ascii", "edgelists")
+ * (Graph/DistributedGraph.hpp:153-172; GraphIngress.hpp:76-304,323-328,511-723).
+ * `flags` = gre_dir | gre_graph_flags.  Arc order: source-major, file order within a source. */
+int gre_graph_load(const char* prefix, uint32_t flags, int device, gre_graph* out);
+/* GraphInCSR::build / rbuild from an edge list in input order (LocalGraph.hpp:66-156). */
+int gre_graph_from_edges(uint64_t n, uint64_t m, const uint32_t* src, const uint32_t* dst,
+                         uint32_t flags, int device, gre_graph* out);
+/* Graph from a CSR (row_off[n+1], col[m]); host or device arrays are copied. */
+int gre_graph_from_csr(uint64_t n, uint64_t m, const uint64_t* row_off, const uint32_t* col,
+                       uint32_t flags, int device, gre_graph* out);
+/* Seeded RMAT graph generated and built on the device (a=.57 b=.19 c=.19), self loops and
+ * duplicates removed; symmetric != 0 adds every reverse arc.  Same arcs as gre_rmat_host. */
+int gre_graph_rmat(uint32_t scale, uint32_t edgefactor, uint64_t seed, int symmetric, int device,
+                   gre_graph* out);
+/* Block-diagonal union of k graphs (ids of graph i shifted by vertex_offset[i], written to
+ * vertex_offset[0..k], host array).  Runs one launch over many graphs of uneven size. */
+int gre_graph_union(const gre_graph* graphs, uint32_t k, int device, gre_graph* out,
+                    uint64_t* vertex_offset);
+int gre_graph_free(gre_graph g);
+/* get_num_masters / get_num_edges (DistributedGraph.hpp:93-110). */
+int gre_graph_info(gre_graph g, uint64_t* n, uint64_t* m, uint32_t* flags);
+/* getOutdegree for every vertex (DistributedGraph.hpp:178-180). */
+int gre_graph_outdegree(gre_graph g, uint32_t* outdeg);
+/* Copy the CSR back (row_off[n+1], col[m]). */
+int gre_graph_csr(gre_graph g, uint64_t* row_off, uint32_t* col);
+/* DistributedGraph::loadEdgeProperty (DistributedGraph.hpp:195-226): uint32 weight per arc in
+ * CSR order.  The CSC copy is derived on the device. */
+int gre_graph_set_weights_u32(gre_graph g, const uint32_t* w);
+/* Weight of arc (u,v) = 1 + H(wseed, min(u,v), max(u,v)) % 255 (gre_sssp_weight), computed
+ * on the device for every arc. */
+int gre_graph_set_weights_hash(gre_graph g, uint64_t wseed);
+/* FP64 weight per arc in CSR order (weighted PageRank and its adjoint). */
+int gre_graph_set_weights_f64(gre_graph g, const double* w);
+
+/* ---------------------------------------------------------------------------------------
+ * Reference-semantics engine: the reference plugins run on a device SynchronousEngine
+ * (frontier bitmap + list, combine through atomics, apply on the nextSet bitmap,
+ * assert_to_halt).  Per-superstep active counts equal the reference's for deterministic
+ * plugins.  `max_supersteps` = configMaxSupersteps (Engine.hpp:148-153; 0 = 1024).
+ * ------------------------------------------------------------------------------------- */
+/* usr/test_pagerank.cpp: PageRank (variant GRE_PR_REFERENCE) or PageRankIter, run<Out>,
+ * srcSet.setALL().  pr: n doubles. */
+int gre_vc_pagerank(gre_graph g, int variant, uint32_t max_supersteps, double* pr, gre_stats* st);
+/* usr/test_bfs.cpp: BFS plugin (Kernels/BFS.hpp), run<dir> from one source.  pred: n uint64
+ * as the plugin leaves it: it forwards pred_scatter = pred (BFS.hpp:66-72), so every reached
+ * vertex holds the source's vid and unreached ones UINT64_MAX; level: n int32, the superstep
+ * in which apply() reached the vertex (the BFS level; -1 unreached).  Either may be NULL. */
+int gre_vc_bfs(gre_graph g, uint32_t src, int dir, uint64_t* pred, int32_t* level, gre_stats* st);
+/* usr/test_sssp.cpp: SSSP plugin (Kernels/SSSP.hpp), run<Out>, graph weights required.
+ * dist: n uint32 (UINT32_MAX unreached). */
+int gre_vc_sssp(gre_graph g, uint32_t src, uint32_t max_supersteps, uint32_t* dist, gre_stats* st);
+/* usr/test_cc.cpp: ConnectedComponents (Kernels/CC.hpp), run<InOut>, setALL.  label: n
+ * uint32 = minimum vid of the component. */
+int gre_vc_cc(gre_graph g, uint32_t* label, gre_stats* st);
+/* usr/test_bc.cpp looped over sources: Forward run<Out> + Backward run<In> per level
+ * (Kernels/BC.hpp); bc[v] = sum over sources s != v of dep_s(v).  bc: n doubles. */
+int gre_vc_bc(gre_graph g, const uint32_t* srcs, uint32_t nsrc, double* bc, gre_stats* st);
+
+/* ---------------------------------------------------------------------------------------
+ * B200 fast paths: same results, kernels shaped for the hardware.
+ * ------------------------------------------------------------------------------------- */
+/* PageRank, pull over in-arcs in FP64, `iters` supersteps, teleport (1-d) (d = 0.85 gives the
+ * reference's 0.15).  pr: n doubles. */
+int gre_pagerank(gre_graph g, int variant, double d, uint32_t iters, double* pr, gre_stats* st);
+/* Direction-optimising BFS, one run per source.  levels: nsrc x n int32 (-1 unreached). */
+int gre_bfs(gre_graph g, const uint32_t* srcs, uint32_t nsrc, int32_t* levels, gre_stats* st);
+/* Multi-source BFS with 64 sources per uint64 frontier word.  levels: nsrc x n int32. */
+int gre_msbfs(gre_graph g, const uint32_t* srcs, uint32_t nsrc, int32_t* levels, gre_stats* st);
+/* One BFS whose level-0 frontier holds all `nroots` roots (distance to the nearest root);
+ * on a gre_graph_union this is one BFS per member graph in a single launch sequence. */
+int gre_bfs_multiroot(gre_graph g, const uint32_t* roots, uint32_t nroots, int32_t* level,
+                      gre_stats* st);
+/* SSSP with uint32 weights, one run per source.  dist: nsrc x n uint32 (UINT32_MAX
+ * unreached).  Graph weights required. */
+int gre_sssp(gre_graph g, const uint32_t* srcs, uint32_t nsrc, uint32_t* dist, gre_stats* st);
+/* Connected components (symmetric graph): label = minimum vid of the component. */
+int gre_cc(gre_graph g, uint32_t* label, gre_stats* st);
+/* Brandes betweenness over nsrc sources, bc[v] = sum over s != v of dep_s(v) (FP64).
+ * batched = 0: one source at a time; batched = 1: 64 sources per uint64 word.  Both give
+ * bit-identical results. */
+int gre_bc(gre_graph g, const uint32_t* srcs, uint32_t nsrc, int batched, double* bc, gre_stats* st);
+/* Personalised PageRank for k one-hot restart vectors: out[i*n+v], x = (1-d)e_seed + d A^T D^-1 x,
+ * `iters` Jacobi steps from x0 = (1-d)e_seed.  batched = 1 runs all k in one pass per step. */
+int gre_ppr(gre_graph g, const uint32_t* seeds, uint32_t k, double d, uint32_t iters, int batched,
+            double* out, gre_stats* st);
+/* Weighted PageRank r = (1-d)pers + d P^T r, P = D_s^-1 W (graph FP64 weights, dangling rows
+ * zero), Jacobi steps from r0 = (1-d)pers until max|r_k+1 - r_k| <= tol or max_iters.
+ * pers: n doubles (NULL = all ones).  r: n doubles. */
+int gre_pagerank_weighted(gre_graph g, double d, const double* pers, double tol, uint32_t max_iters,
+                          double* r, gre_stats* st);
+/* Adjoint of gre_pagerank_weighted for L = c^T r, given the converged r:
+ * lambda = c + d P lambda (same tolerance rule); grad_pers = (1-d) lambda;
+ * grad_w[arc u->v] = d r_u / s_u (lambda_v - sum_k P_uk lambda_k) in CSR order.
+ * lambda and grad_pers: n doubles (either may be NULL); grad_w: m doubles. */
+int gre_pagerank_adjoint(gre_graph g, double d, const double* r, const double* c, double tol,
+                         uint32_t max_iters, double* lambda, double* grad_pers, double* grad_w,
+                         gre_stats* st);
+
+/* ---------------------------------------------------------------------------------------
+ * Host utilities (CPU only, no GPU needed).
+ * ------------------------------------------------------------------------------------- */
+/* RMAT CSR on the host (same arcs as gre_graph_rmat).  *row_off and *col are malloc'ed;
+ * release with gre_host_free. */
+int gre_rmat_host(uint32_t scale, uint32_t edgefactor, uint64_t seed, int symmetric, uint64_t* n,
+                  uint64_t* m, uint64_t** row_off, uint32_t** col);
+void gre_host_free(void* p);
+/* Write <prefix>.meta and <prefix>.edges.<i>, i < nfiles, source u in file u % nfiles. */
+int gre_write_edgelists(const char* prefix, uint64_t n, uint64_t m, const uint64_t* row_off,
+                        const uint32_t* col, uint32_t nfiles);
+/* <prefix>.roots: "count\n v1\n v2 ..." (read by Util::loadFromFile, Util/Util.hpp:140-157). */
+int gre_write_roots(const char* prefix, const uint32_t* roots, uint32_t count);
+int gre_read_roots(const char* prefix, uint32_t* roots, uint32_t capacity, uint32_t* count);
+/* The SSSP weight function of gre_graph_set_weights_hash. */
+uint32_t gre_sssp_weight(uint64_t wseed, uint32_t u, uint32_t v);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GRE_GPU_H */

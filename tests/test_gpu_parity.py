@@ -1,0 +1,340 @@
+"""GPU parity: every entry point of libgre_gpu.so against the oracle.
+
+* golden fixtures (outputs of the reference GRE engine, tests/golden/): bit-exact for BFS levels,
+  SSSP distances, CC labels and per-superstep active counts; FP64 results within 1e-9 relative L1;
+* seeded RMAT graphs up to scale 16 against the C++ restatement (oracle/gre_oracle.cpp);
+* scale-20 graphs through size-independent properties (BFS level consistency, SSSP
+  tightness, CC closure) that the oracle cannot afford at that size in a test.
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import graphine_b200.gre as G
+import oracle as O
+from conftest import golden_cases, rel_l1
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-9  # FP64 relative L1
+CASES = golden_cases()
+SYM = [c for c in CASES if not c.endswith("dir")]
+
+
+def graph_of(case):
+    sym = bool(case["symmetric"])
+    return G.Graph.from_csr(int(case["n"]), case["off"], case["col"], dir=G.InOut if sym else G.Out, symmetric=sym)
+
+
+# ---------------------------------------------------------------------------------------------
+# golden fixtures (reference outputs)
+# ---------------------------------------------------------------------------------------------
+@pytest.mark.parametrize("name", CASES)
+def test_pagerank_golden(golden, name):
+    case = golden[name]
+    g = graph_of(case)
+    pr, st = G.vc_pagerank(g, G.PR_REFERENCE, 10)
+    assert rel_l1(pr, case["pr_gre10"]) <= TOL
+    assert st.supersteps == 10 and st.active == list(case["pr_gre10_active"])
+    pr, st = G.vc_pagerank(g, G.PR_ITER, 20)
+    assert rel_l1(pr, case["pr_iter20"]) <= TOL
+    assert st.active == list(case["pr_iter20_active"])
+    pr, _ = G.pagerank(g, G.PR_REFERENCE, 0.85, 10)
+    assert rel_l1(pr, case["pr_gre10"]) <= TOL
+    pr, _ = G.pagerank(g, G.PR_ITER, 0.85, 20)
+    assert rel_l1(pr, case["pr_iter20"]) <= TOL
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("batched", [False, True])
+def test_ppr_golden(golden, name, batched):
+    case = golden[name]
+    g = graph_of(case)
+    out, _ = G.ppr(g, case["roots"][:2], 0.85, 20, batched=batched)
+    assert rel_l1(out, case["ppr20"].ravel()) <= TOL
+
+
+@pytest.mark.parametrize("name", SYM)
+def test_bfs_golden(golden, name):
+    case = golden[name]
+    g = graph_of(case)
+    roots = case["roots"]
+    for i, r in enumerate(roots):
+        pred, level, st = G.vc_bfs(g, int(r), G.In)
+        np.testing.assert_array_equal(level, case["bfs_level"][i])
+        assert st.active == [x for x in case["bfs_active"][i] if x >= 0]
+        assert np.all((pred == int(r)) == (level >= 0))
+        lv, st = G.bfs(g, [r])
+        np.testing.assert_array_equal(lv, case["bfs_level"][i])
+        assert st.active == [x for x in case["bfs_active"][i] if x >= 0]
+    lv, _ = G.msbfs(g, roots)
+    np.testing.assert_array_equal(lv.reshape(len(roots), -1), case["bfs_level"])
+    lv, _ = G.bfs(g, roots)
+    np.testing.assert_array_equal(lv.reshape(len(roots), -1), case["bfs_level"])
+
+
+@pytest.mark.parametrize("name", SYM)
+def test_sssp_golden(golden, name):
+    case = golden[name]
+    g = graph_of(case)
+    g.set_weights_hash(int(case["wseed"]))
+    for i, r in enumerate(case["roots"]):
+        dist, st, status = G.vc_sssp(g, int(r))
+        assert status == G.GRE_SUCCESS
+        np.testing.assert_array_equal(dist, case["sssp_dist"][i])
+        assert st.active == [x for x in case["sssp_active"][i] if x >= 0]
+    dist, _ = G.sssp(g, case["roots"])
+    np.testing.assert_array_equal(dist.reshape(len(case["roots"]), -1), case["sssp_dist"])
+
+
+@pytest.mark.parametrize("name", SYM)
+def test_cc_golden(golden, name):
+    case = golden[name]
+    g = graph_of(case)
+    lab, st = G.vc_cc(g)
+    np.testing.assert_array_equal(lab, case["cc_label"])
+    assert st.active == list(case["cc_active"])
+    lab, _ = G.cc(g)
+    np.testing.assert_array_equal(lab, case["cc_label"])
+
+
+@pytest.mark.parametrize("name", SYM)
+def test_bc_golden(golden, name):
+    case = golden[name]
+    g = graph_of(case)
+    b, _ = G.vc_bc(g, case["roots"])
+    assert rel_l1(b, case["bc"]) <= TOL
+    b1, _ = G.bc(g, case["roots"], batched=False)
+    b2, _ = G.bc(g, case["roots"], batched=True)
+    assert rel_l1(b1, case["bc"]) <= TOL
+    np.testing.assert_array_equal(b1, b2)  # batched and looped: identical bits
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_loader_matches_fixture(golden, name):
+    """gre_graph_load on the text files gives the fixture's CSR (file order within a source)."""
+    case = golden[name]
+    if name.startswith("toy"):
+        pytest.skip("hand-written text; covered by the oracle tests")
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "g")
+        G.write_edgelists(p, int(case["n"]), case["off"], case["col"], 4)
+        g = G.Graph.ingress(p, G.InOut)
+    off, col = g.csr()
+    np.testing.assert_array_equal(off, case["off"])
+    np.testing.assert_array_equal(col, case["col"])
+    np.testing.assert_array_equal(g.getOutdegree(), np.diff(case["off"].astype(np.int64)))
+
+
+# ---------------------------------------------------------------------------------------------
+# seeded RMAT vs the restatement
+# ---------------------------------------------------------------------------------------------
+@pytest.fixture(scope="module")
+def rmat14():
+    n, off, col = G.rmat_host(14, 16, 42, True)
+    g = G.Graph.from_csr(n, off, col, dir=G.InOut, symmetric=True)
+    R = O.Restatement.from_csr(n, off, col)
+    roots = G.sample_sources(off, 16, 9)
+    return n, off, col, g, R, roots
+
+
+def test_rmat14_device_generator_matches_host():
+    n, off, col = G.rmat_host(14, 16, 42, True)
+    g = G.Graph.rmat(14, 16, 42, True)
+    o2, c2 = g.csr()
+    np.testing.assert_array_equal(o2, off)
+    np.testing.assert_array_equal(c2, col)
+    n, off, col = G.rmat_host(13, 8, 5, False)
+    g = G.Graph.rmat(13, 8, 5, False)
+    o2, c2 = g.csr()
+    np.testing.assert_array_equal(o2, off)
+    np.testing.assert_array_equal(c2, col)
+
+
+def test_rmat14_bfs(rmat14):
+    n, off, col, g, R, roots = rmat14
+    ref = R.bfs_many(roots)
+    lv, st = G.bfs(g, roots)
+    np.testing.assert_array_equal(lv.reshape(len(roots), n), ref)
+    lv, _ = G.msbfs(g, roots)
+    np.testing.assert_array_equal(lv.reshape(len(roots), n), ref)
+    assert st.traversed_edges > 0
+
+
+def test_rmat14_sssp(rmat14):
+    n, off, col, g, R, roots = rmat14
+    g.set_weights_hash(77)
+    ref = R.sssp_many(roots, 77)
+    d, _ = G.sssp(g, roots)
+    np.testing.assert_array_equal(d.reshape(len(roots), n), ref)
+    d0, _, _ = G.vc_sssp(g, int(roots[0]))
+    np.testing.assert_array_equal(d0, ref[0])
+
+
+def test_rmat14_cc(rmat14):
+    n, off, col, g, R, roots = rmat14
+    ref, _ = R.cc()
+    lab, _ = G.cc(g)
+    np.testing.assert_array_equal(lab, ref)
+    lab, _ = G.vc_cc(g)
+    np.testing.assert_array_equal(lab, ref)
+
+
+def test_rmat14_pagerank(rmat14):
+    n, off, col, g, R, roots = rmat14
+    for variant, ss in [(0, 10), (1, 20)]:
+        ref, _ = R.pagerank(variant, 0.85, ss)
+        pr, _ = G.pagerank(g, variant, 0.85, ss)
+        assert rel_l1(pr, ref) <= TOL
+        pr, _ = G.vc_pagerank(g, variant, ss)
+        assert rel_l1(pr, ref) <= TOL
+
+
+def test_rmat14_bc_batched_equals_looped(rmat14):
+    n, off, col, g, R, roots = rmat14
+    srcs = G.sample_sources(off, 70, 3)  # more than one 64-source word
+    ref, ovf = R.bc(srcs)
+    b1, _ = G.bc(g, srcs, batched=False)
+    b2, _ = G.bc(g, srcs, batched=True)
+    np.testing.assert_array_equal(b1, b2)
+    assert rel_l1(b2, ref) <= TOL
+
+
+def test_rmat14_ppr(rmat14):
+    n, off, col, g, R, roots = rmat14
+    seeds = roots[:5]
+    ref = R.ppr(seeds, 0.85, 20)
+    a, _ = G.ppr(g, seeds, 0.85, 20, batched=True)
+    b, _ = G.ppr(g, seeds, 0.85, 20, batched=False)
+    assert rel_l1(a, ref.ravel()) <= TOL
+    assert rel_l1(b, ref.ravel()) <= TOL
+
+
+def test_directed_pagerank_s16():
+    n, off, col = G.rmat_host(16, 16, 1, False)
+    g = G.Graph.from_csr(n, off, col, dir=G.Out)
+    R = O.Restatement.from_csr(n, off, col)
+    for variant, ss in [(0, 20), (1, 20)]:
+        ref, _ = R.pagerank(variant, 0.85, ss)
+        pr, st = G.pagerank(g, variant, 0.85, ss)
+        assert rel_l1(pr, ref) <= TOL
+        assert st.traversed_edges == g.m * ss
+
+
+# ---------------------------------------------------------------------------------------------
+# device buffers, errors
+# ---------------------------------------------------------------------------------------------
+def test_device_buffers_roundtrip(rmat14):
+    import torch
+
+    n, off, col, g, R, roots = rmat14
+    out = torch.empty(n, dtype=torch.int32, device="cuda")
+    G.bfs(g, torch.tensor(roots[:1].astype(np.int32), device="cuda"), out=out)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(out.cpu().numpy(), R.bfs(int(roots[0]))[0])
+    pr = torch.empty(n, dtype=torch.float64, device="cuda")
+    G.pagerank(g, G.PR_ITER, 0.85, 20, out=pr)
+    torch.cuda.synchronize()
+    ref, _ = R.pagerank(1, 0.85, 20)
+    assert rel_l1(pr.cpu().numpy(), ref) <= TOL
+
+
+def test_errors_are_status_codes(rmat14):
+    n, off, col, g, R, roots = rmat14
+    with pytest.raises(G.GreError) as e:
+        G.bfs(g, [n + 5])
+    assert e.value.status == G.GRE_INVALID_ARG
+    g2 = G.Graph.from_csr(n, off, col, dir=G.InOut, symmetric=True)
+    with pytest.raises(G.GreError) as e:
+        G.sssp(g2, [0])  # no weights
+    assert e.value.status == G.GRE_INVALID_ARG
+    with pytest.raises(G.GreError) as e:
+        G.pagerank(g2, 7)
+    assert e.value.status == G.GRE_INVALID_ARG
+
+
+# ---------------------------------------------------------------------------------------------
+# batch of uneven graphs in one launch (block-diagonal union)
+# ---------------------------------------------------------------------------------------------
+def test_graph_union_batch():
+    parts = []
+    for i, s in enumerate([10, 12, 9, 11]):
+        n, off, col = G.rmat_host(s, 16, 100 + i, True)
+        parts.append((n, off, col))
+    gs = [G.Graph.from_csr(n, o, c, dir=G.InOut, symmetric=True) for n, o, c in parts]
+    for g in gs:
+        g.set_weights_hash(5)
+    U, voff = G.Graph.union(gs)
+    assert U.n == sum(p[0] for p in parts) and U.symmetric
+    roots = [int(G.sample_sources(p[1], 1, 1)[0]) for p in parts]
+    lv, _ = G.bfs_multiroot(U, [r + int(voff[i]) for i, r in enumerate(roots)])
+    lab, _ = G.cc(U)
+    pr, _ = G.pagerank(U, G.PR_ITER, 0.85, 20)
+    for i, (n, off, col) in enumerate(parts):
+        a, b = int(voff[i]), int(voff[i + 1])
+        R = O.Restatement.from_csr(n, off, col)
+        np.testing.assert_array_equal(lv[a:b], R.bfs(roots[i])[0])
+        ref_lab, _ = R.cc()
+        np.testing.assert_array_equal(lab[a:b] - a, ref_lab)
+        ref_pr, _ = R.pagerank(1, 0.85, 20)
+        assert rel_l1(pr[a:b], ref_pr) <= TOL
+
+
+# ---------------------------------------------------------------------------------------------
+# scale 20: size-independent properties
+# ---------------------------------------------------------------------------------------------
+@pytest.fixture(scope="module")
+def rmat20():
+    g = G.Graph.rmat(20, 16, 2024, True)
+    off, col = g.csr()
+    src = np.repeat(np.arange(g.n, dtype=np.int64), np.diff(off.astype(np.int64)))
+    return g, off, col, src
+
+
+def test_s20_bfs_properties(rmat20):
+    g, off, col, src = rmat20
+    roots = G.sample_sources(off, 2, 4)
+    lv, _ = G.bfs(g, roots)
+    lv = lv.reshape(len(roots), g.n)
+    lv2, _ = G.msbfs(g, roots)
+    np.testing.assert_array_equal(lv2.reshape(len(roots), g.n), lv)
+    for i, r in enumerate(roots):
+        L = lv[i].astype(np.int64)
+        assert L[r] == 0
+        a, b = L[src], L[col]
+        reached = a >= 0
+        assert np.all((b >= 0)[reached])  # a reached vertex's neighbours are reached
+        assert np.all(np.abs(a[reached] - b[reached]) <= 1)
+        # every reached vertex other than the root has a neighbour one level up
+        has_parent = np.zeros(g.n, dtype=bool)
+        has_parent[col[(b == a + 1) & reached]] = True
+        assert np.all(has_parent[(L > 0)])
+
+
+def test_s20_sssp_properties(rmat20):
+    g, off, col, src = rmat20
+    g.set_weights_hash(31)
+    r = int(G.sample_sources(off, 1, 8)[0])
+    d, _ = G.sssp(g, [r])
+    lo = np.minimum(src, col).astype(np.uint64)
+    hi = np.maximum(src, col).astype(np.uint64)
+    # weights recomputed on the host through the oracle's independent restatement
+    wt = np.array([O.sssp_weight(31, int(u), int(v)) for u, v in zip(lo[:2000], hi[:2000])], dtype=np.int64)
+    du, dv = d[src].astype(np.int64), d[col].astype(np.int64)
+    inf = 0xFFFFFFFF
+    sel = (du[:2000] != inf)
+    assert np.all(dv[:2000][sel] <= du[:2000][sel] + wt[sel])
+    dl, _ = G.bfs(g, [r])
+    assert np.all((d == inf) == (dl < 0))
+
+
+def test_s20_cc_properties(rmat20):
+    g, off, col, src = rmat20
+    lab, _ = G.cc(g)
+    assert np.all(lab[src] == lab[col])
+    assert np.all(lab <= np.arange(g.n))
+    assert np.all(lab[lab] == lab)
+    lab2, _ = G.vc_cc(g)
+    np.testing.assert_array_equal(lab, lab2)
