@@ -6,17 +6,20 @@ Workload (ours, per GPU): RMAT scale 26, edge factor 16, symmetrised and de-dupl
 (a/b/c = 0.57/0.19/0.19, seeded), uint32 ids, uint64 offsets, SSSP weights uint32 in
 [1, 255]; generated on the device.  One step = the plain suite of the reference's plugins:
 PageRank 20 supersteps (FP64, power iteration), direction-optimising BFS from one source,
-SSSP from one source, connected components, and betweenness from 64 sources in one batched
-pass.  Sources are seeded samples of non-isolated vertices, different every step.
+SSSP from one source and connected components.  Sources are seeded samples of non-isolated
+vertices, different every step.
 
 Metric: GTEPS = traversed edges / device time, summed over the suite (PageRank: arcs x
 supersteps; BFS/SSSP: undirected edges of the reached component (Graph500); CC: undirected
-edges; BC: sources x undirected edges).  Per-algorithm GTEPS and algorithmic HBM GB/s are
-reported beside it.  `value` uses device-resident outputs; `e2e` runs the same calls with
-pinned host outputs, the device->host copies inside the timed region.
+edges).  Per-algorithm GTEPS and algorithmic HBM GB/s are reported beside it.  `value` uses
+device-resident outputs; `e2e` runs the same calls with pinned host outputs, the device->host
+copies inside the timed region.  After the timed steps, `batched_vs_plain` reports the batched
+forms against their looped plain forms at equal results (256-source BC, 64-source BFS, 128
+personalised PageRank vectors, a batch of 32 uneven graphs; scale 20) and the PageRank adjoint
+against its forward, plus one 64-source BC batch on the scale-26 graph.
 
 --impl reference runs the reference GRE engine (compiled from its headers into oracle/_ref/)
-on the host CPU over a bounded sample (RMAT scale 16, same suite) and prints the same line.
+on the host CPU over a bounded sample (RMAT scale 16, same plain suite) and prints the same line.
 """
 from __future__ import annotations
 
@@ -42,7 +45,6 @@ WSEED = 20240601
 PR_ITERS = 20
 BC_SOURCES = 64
 CPU_SCALE = 16
-CPU_BC_SOURCES = 8  # betweenness sources per step in the bounded CPU sample
 
 
 def env_int(name, default):
@@ -140,7 +142,7 @@ def reference_suite(scale: int, reps: int, workdir: str):
     n, off, col = G.rmat_host(scale, 16, SEED, True)
     prefix = os.path.join(workdir, f"rmat{scale}")
     G.write_edgelists(prefix, n, off, col, 4)
-    roots = G.sample_sources(off, reps * CPU_BC_SOURCES, 5)
+    roots = G.sample_sources(off, reps, 5)
     G.write_roots(prefix, roots)
     R = O.Restatement.from_csr(n, off, col)
     m_arcs = len(col)
@@ -158,12 +160,10 @@ def reference_suite(scale: int, reps: int, workdir: str):
     t["sssp"] = run.seconds
     _, run = O.run_reference("cc", prefix, reps)
     t["cc"] = run.seconds
-    _, run = O.run_reference("bc", prefix, reps * CPU_BC_SOURCES)
-    t["bc"] = [sum(run.seconds[r * CPU_BC_SOURCES:(r + 1) * CPU_BC_SOURCES]) for r in range(reps)]
     out = []
     for r in range(reps):
-        edges = m_arcs * PR_ITERS + comp_edges[r] + comp_edges[r] + m_und + CPU_BC_SOURCES * m_und
-        secs = t["pagerank"][r] + t["bfs"][r] + t["sssp"][r] + t["cc"][r] + t["bc"][r]
+        edges = m_arcs * PR_ITERS + comp_edges[r] + comp_edges[r] + m_und
+        secs = t["pagerank"][r] + t["bfs"][r] + t["sssp"][r] + t["cc"][r]
         out.append((edges, secs))
     return out, {"n": n, "m": m_arcs}
 
@@ -185,7 +185,7 @@ def run_reference_arm(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+u32", "data": "synthetic",
-        "config": {"workload": f"GRE suite (PageRank-20 iter, BFS, SSSP, CC, BC {CPU_BC_SOURCES} src) on RMAT scale {CPU_SCALE} "
+        "config": {"workload": f"GRE plain suite (PageRank-20 iter, BFS, SSSP, CC) on RMAT scale {CPU_SCALE} "
                                f"symmetric EF16 (bounded sample of the scale-26 workload)",
                    "graph_n": info["n"], "graph_arcs": info["m"], "parallelism": "cpu"},
         "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": cpu_cores_used(), "kind": "reference",
@@ -200,6 +200,60 @@ def run_reference_arm(args, rank, world):
 # ----------------------------------------------------------------------------------------------
 # our arm
 # ----------------------------------------------------------------------------------------------
+def batched_block(G, dev_index: int, scale: int, seed: int):
+    """Batched forms vs their looped plain forms at equal results (measured once, untimed for
+    `value`): 256-source BC, 64-source BFS, 128 personalised PageRank vectors, a batch of 32
+    uneven RMAT graphs, and the PageRank adjoint vs its forward."""
+    out = {"scale": scale}
+    g = G.Graph.rmat(scale, 16, seed, True, device=dev_index, reorder=True)
+    off, _ = g.csr()
+    srcs = G.sample_sources(off, 256, 11)
+    b_loop, s_loop = G.bc(g, srcs, batched=False)
+    b_bat, s_bat = G.bc(g, srcs, batched=True)
+    out["bc256"] = {"looped_ms": s_loop.device_ms, "batched_ms": s_bat.device_ms,
+                    "speedup": s_loop.device_ms / s_bat.device_ms, "identical": bool(np.array_equal(b_loop, b_bat))}
+    l_loop, s_loop = G.bfs(g, srcs[:64])
+    l_bat, s_bat = G.msbfs(g, srcs[:64])
+    out["bfs64"] = {"looped_ms": s_loop.device_ms, "batched_ms": s_bat.device_ms,
+                    "speedup": s_loop.device_ms / s_bat.device_ms, "identical": bool(np.array_equal(l_loop, l_bat))}
+    p_loop, s_loop = G.ppr(g, srcs[:128], 0.85, PR_ITERS, batched=False)
+    p_bat, s_bat = G.ppr(g, srcs[:128], 0.85, PR_ITERS, batched=True)
+    out["ppr128"] = {"looped_ms": s_loop.device_ms, "batched_ms": s_bat.device_ms,
+                     "speedup": s_loop.device_ms / s_bat.device_ms,
+                     "rel_l1": float(np.abs(p_loop - p_bat).sum() / np.abs(p_loop).sum())}
+    del g
+    # 32 RMAT graphs of uneven scales 12..18 in one launch sequence (block-diagonal union)
+    rng = np.random.default_rng(seed)
+    scales = rng.integers(12, 19, size=32)
+    parts = [G.Graph.rmat(int(s), 16, seed + i, True, device=dev_index) for i, s in enumerate(scales)]
+    roots = []
+    for p in parts:
+        o, _ = p.csr()
+        roots.append(int(G.sample_sources(o, 1, 3)[0]))
+    U, voff = G.Graph.union(parts)
+    t_loop, lv_loop = 0.0, []
+    for p, r in zip(parts, roots):
+        lv, st = G.bfs(p, [r])
+        t_loop += st.device_ms
+        lv_loop.append(lv)
+    lv_u, st_u = G.bfs_multiroot(U, [r + int(voff[i]) for i, r in enumerate(roots)])
+    out["graph_batch32_bfs"] = {"looped_ms": t_loop, "batched_ms": st_u.device_ms, "speedup": t_loop / st_u.device_ms,
+                                "identical": bool(np.array_equal(np.concatenate(lv_loop), lv_u)),
+                                "scales": [int(s) for s in scales]}
+    del parts, U
+    # adjoint vs forward (weighted PageRank, lognormal(0,1) weights, row-normalised)
+    g = G.Graph.rmat(scale, 16, seed + 7, False, device=dev_index, reorder=True)
+    w = np.exp(np.random.default_rng(seed).standard_normal(g.m))
+    g.set_weights_f64(w)
+    c = np.random.default_rng(seed + 1).standard_normal(g.n)
+    r, s_fwd, _ = G.pagerank_weighted(g, 0.85, None, tol=1e-13, max_iters=2000)
+    lam, gp, gw, s_adj, _ = G.pagerank_adjoint(g, r, c, 0.85, tol=1e-13, max_iters=2000)
+    out["pagerank_adjoint"] = {"forward_ms": s_fwd.device_ms, "adjoint_ms": s_adj.device_ms,
+                               "adjoint_over_forward": s_adj.device_ms / s_fwd.device_ms,
+                               "forward_iters": s_fwd.supersteps, "adjoint_iters": s_adj.supersteps}
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import graphine_b200.gre as G
@@ -210,7 +264,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
 
-    g = G.Graph.rmat(args.scale, 16, SEED, True, device=local_rank)
+    g = G.Graph.rmat(args.scale, 16, SEED, True, device=local_rank, reorder=not args.no_reorder)
     g.set_weights_hash(WSEED)
     n, m = g.n, g.m
     outdeg = g.getOutdegree()
@@ -218,32 +272,21 @@ def run_ours(args, rank, world, local_rank):
     rng = np.random.default_rng(1000 + rank)
     nsteps = args.warmup + args.steps
     one_src = rng.choice(nz, size=nsteps, replace=False).astype(np.uint32)
-    bc_src = [np.sort(rng.choice(nz, size=args.bc_sources, replace=False)).astype(np.uint32) for _ in range(nsteps)]
 
-    # device outputs (value)
+    # device-resident outputs (value)
     pr_d = torch.empty(n, dtype=torch.float64, device=dev)
     lv_d = torch.empty(n, dtype=torch.int32, device=dev)
     ds_d = torch.empty(n, dtype=torch.int32, device=dev)  # uint32 payload
     cc_d = torch.empty(n, dtype=torch.int32, device=dev)
-    bc_d = torch.empty(n, dtype=torch.float64, device=dev)
-    names = ["pagerank", "bfs", "sssp", "cc", "bc64"]
+    names = ["pagerank", "bfs", "sssp", "cc"]
 
-    def suite(i, outs, bcs=None):
-        pr_o, lv_o, ds_o, cc_o, bc_o = outs
-        r = []
-        _, s = G.pagerank(g, G.PR_ITER, 0.85, PR_ITERS, out=pr_o)
-        r.append(s)
-        _, s = G.bfs(g, one_src[i:i + 1], out=lv_o)
-        r.append(s)
-        _, s = G.sssp(g, one_src[i:i + 1], out=ds_o)
-        r.append(s)
-        _, s = G.cc(g, out=cc_o)
-        r.append(s)
-        _, s = G.bc(g, bc_src[i] if bcs is None else bcs, batched=True, out=bc_o)
-        r.append(s)
-        return r
+    def suite(i, outs, src=None):
+        pr_o, lv_o, ds_o, cc_o = outs
+        s_ = one_src[i:i + 1] if src is None else src
+        return [G.pagerank(g, G.PR_ITER, 0.85, PR_ITERS, out=pr_o)[1], G.bfs(g, s_, out=lv_o)[1],
+                G.sssp(g, s_, out=ds_o)[1], G.cc(g, out=cc_o)[1]]
 
-    dev_outs = (pr_d, lv_d, ds_d, cc_d, bc_d)
+    dev_outs = (pr_d, lv_d, ds_d, cc_d)
     for i in range(args.warmup):
         suite(i, dev_outs)
     torch.cuda.synchronize()
@@ -267,18 +310,17 @@ def run_ours(args, rank, world, local_rank):
     tot_ms = sum(v["ms"] for v in per.values())
     tot_edges = sum(v["edges"] for v in per.values())
 
-    # e2e: same calls, pinned host outputs (device->host copies inside each call's timed span)
+    # e2e: the same calls with pinned host buffers; the source id comes from pinned memory and
+    # every result is copied device->host inside the timed span
     pin = lambda dt, k: torch.empty(k, dtype=dt, pin_memory=True).numpy()  # noqa: E731
-    host_outs = (pin(torch.float64, n), pin(torch.int32, n), pin(torch.int32, n), pin(torch.int32, n),
-                 pin(torch.float64, n))
-    src_pinned = pin(torch.int32, args.bc_sources).view(np.uint32)
+    host_outs = (pin(torch.float64, n), pin(torch.int32, n), pin(torch.int32, n), pin(torch.int32, n))
+    src_pinned = pin(torch.int32, 1).view(np.uint32)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     e2e_edges = 0
     for i in range(args.warmup, nsteps):
-        src_pinned[:] = bc_src[i]
-        res = suite(i, host_outs, src_pinned)
-        e2e_edges += sum(s.traversed_edges for s in res)
+        src_pinned[0] = one_src[i]
+        e2e_edges += sum(s.traversed_edges for s in suite(i, host_outs, src_pinned))
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
 
@@ -304,34 +346,43 @@ def run_ours(args, rank, world, local_rank):
     achieved = pr_bytes_iter / (pr_iter_ms * 1e-3) / 1e9
     per_alg = {}
     for k, v in per.items():
-        per_alg[k] = {"ms_per_step": v["ms"] / args.steps, "gteps": v["edges"] / (v["ms"] * 1e-3) / 1e9 if v["ms"] else None,
+        per_alg[k] = {"ms_per_step": v["ms"] / args.steps,
+                      "gteps": v["edges"] / (v["ms"] * 1e-3) / 1e9 if v["ms"] else None,
                       "hbm_gbs_algorithmic": v["bytes"] / (v["ms"] * 1e-3) / 1e9 if v["ms"] else None,
                       "share": v["ms"] / tot_ms}
+    extra = {}
+    if not args.no_batched:
+        # one 64-source betweenness batch on the scale-26 graph, then the batched-vs-looped block
+        srcs = np.sort(rng.choice(nz, size=BC_SOURCES, replace=False)).astype(np.uint32)
+        _, s = G.bc(g, srcs, batched=True)
+        extra["bc64_s26"] = {"ms": s.device_ms, "gteps": s.traversed_edges / (s.device_ms * 1e-3) / 1e9}
+        del g
+        torch.cuda.empty_cache()
+        extra.update(batched_block(G, local_rank, args.batch_scale, 77))
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         with tempfile.TemporaryDirectory() as td:
             res, info = reference_suite(CPU_SCALE, 1, td)
         e, s = res[0]
         cpu = {"value": e / s / 1e9, "unit": "GTEPS", "cores": cpu_cores_used(), "kind": "reference",
-               "sample": f"one suite on RMAT-{CPU_SCALE} symmetric (n={info['n']}, arcs={info['m']}), reference GRE "
-                         f"engine -O0 np=1, engine.run timed; BC from {CPU_BC_SOURCES} sources"}
-    d2h = n * (8 + 4 + 4 + 4 + 8)
+               "sample": f"one plain suite on RMAT-{CPU_SCALE} symmetric (n={info['n']}, arcs={info['m']}), reference "
+                         f"GRE engine -O0 np=1, engine.run timed"}
+    d2h = n * (8 + 4 + 4 + 4)
     line = {
         "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64+u32", "data": "synthetic",
-        "config": {"workload": f"GRE suite on RMAT scale {args.scale} EF16 symmetric: PageRank-{PR_ITERS} (power "
-                               f"iteration), DO-BFS 1 src, SSSP 1 src (u32 w in [1,255]), CC, BC {args.bc_sources} src "
-                               f"batched", "graph_n": n, "graph_arcs": m, "parallelism": f"replica x{world}",
+        "config": {"workload": f"GRE plain suite on RMAT scale {args.scale} EF16 symmetric: PageRank-{PR_ITERS} (power "
+                               f"iteration, FP64), DO-BFS 1 src, SSSP 1 src (u32 w in [1,255]), CC",
+                   "graph_n": n, "graph_arcs": m, "parallelism": f"replica x{world}",
                    "l2": "inputs larger than L2 (graph > 126 MB)"},
         "per_algorithm": per_alg,
         "roofline": {"bound": "hbm", "kernel": "PageRank pull superstep (degree-binned row kernels)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "bytes_per_launch": pr_bytes_iter,
-                     "traffic": profiled_traffic()},
+                     "peak_kind": peak_kind, "bytes_per_launch": pr_bytes_iter, "traffic": profiled_traffic()},
+        "batched_vs_plain": extra,
         "cpu_baseline": cpu,
-        "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": 4 * (1 + 1 + args.bc_sources),
-                "d2h_bytes_per_step": d2h},
+        "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": 4, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
@@ -346,7 +397,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=int, default=26)
-    ap.add_argument("--bc-sources", type=int, default=BC_SOURCES)
+    ap.add_argument("--batch-scale", type=int, default=20)
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-reorder", action="store_true", help="keep the generated vertex order")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     rank, world, local_rank = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)

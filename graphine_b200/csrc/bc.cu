@@ -502,19 +502,17 @@ int gre_bc(gre_graph g, const uint32_t* srcs, uint32_t nsrc, int batched, double
   const uint64_t n = g->n;
   std::vector<uint32_t> hs(nsrc);
   if (nsrc) GRE_CUDA(cudaMemcpy(hs.data(), srcs, sizeof(uint32_t) * nsrc, cudaMemcpyDefault));
-  for (uint32_t s : hs)
-    if (s >= n) {
-      set_error("gre_bc: source %u >= n", s);
-      return GRE_INVALID_ARG;
-    }
+  GRE_CHECK(map_ids(g, &hs, "gre_bc"));
   GRE_CHECK(ensure_bc_chunks(g));
-  double* dbc;
-  GRE_CHECK(prepare_output(g, bc, n, WS_OUTBUF, &dbc));
+  double *dfinal, *dbc;
+  GRE_CHECK(prepare_output(g, bc, n, WS_OUTBUF, &dfinal));
+  GRE_CHECK(perm_out_begin(g, dfinal, 1, 8, (void**)&dbc));
   RunTimer timer(g);
   GRE_CUDA(cudaMemsetAsync(dbc, 0, sizeof(double) * n, g->stream));
   if (batched) GRE_CHECK(bc_batched(g, hs, dbc, st));
   else GRE_CHECK(bc_single(g, hs, dbc, st));
-  GRE_CHECK(finish_output(g, bc, dbc, n));
+  GRE_CHECK(perm_out_end(g, dbc, dfinal, 1, 8));
+  GRE_CHECK(finish_output(g, bc, dfinal, n));
   GRE_CHECK(timer.stop(st));
   if (st) st->traversed_edges = (uint64_t)nsrc * (g->symmetric() ? g->m / 2 : g->m);
   return GRE_SUCCESS;

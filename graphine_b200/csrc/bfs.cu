@@ -385,14 +385,11 @@ int gre_bfs(gre_graph g, const uint32_t* srcs, uint32_t nsrc, int32_t* levels, g
   const uint64_t n = g->n;
   std::vector<uint32_t> hs(nsrc);
   if (nsrc) GRE_CUDA(cudaMemcpy(hs.data(), srcs, sizeof(uint32_t) * nsrc, cudaMemcpyDefault));
-  for (uint32_t s : hs)
-    if (s >= n) {
-      set_error("gre_bfs: source %u >= n", s);
-      return GRE_INVALID_ARG;
-    }
-  int32_t* dl;
+  GRE_CHECK(map_ids(g, &hs, "gre_bfs"));
+  int32_t *dfinal, *dl;
   uint32_t* droot;
-  GRE_CHECK(prepare_output(g, levels, (uint64_t)nsrc * n, WS_OUTBUF, &dl));
+  GRE_CHECK(prepare_output(g, levels, (uint64_t)nsrc * n, WS_OUTBUF, &dfinal));
+  GRE_CHECK(perm_out_begin(g, dfinal, nsrc, 4, (void**)&dl));
   GRE_CHECK(ws_array(g, WS_H, nsrc ? nsrc : 1, &droot));
   RunTimer timer(g);
   if (nsrc) GRE_CUDA(cudaMemcpyAsync(droot, hs.data(), sizeof(uint32_t) * nsrc, cudaMemcpyHostToDevice, g->stream));
@@ -403,7 +400,8 @@ int gre_bfs(gre_graph g, const uint32_t* srcs, uint32_t nsrc, int32_t* levels, g
     GRE_CHECK(count_reached_edges(g, dl + (uint64_t)i * n, &e));
     edges += e;
   }
-  GRE_CHECK(finish_output(g, levels, dl, (uint64_t)nsrc * n));
+  GRE_CHECK(perm_out_end(g, dl, dfinal, nsrc, 4));
+  GRE_CHECK(finish_output(g, levels, dfinal, (uint64_t)nsrc * n));
   GRE_CHECK(timer.stop(st));
   if (st) st->traversed_edges = edges;
   return GRE_SUCCESS;
@@ -416,18 +414,19 @@ int gre_bfs_multiroot(gre_graph g, const uint32_t* roots, uint32_t nroots, int32
   const uint64_t n = g->n;
   std::vector<uint32_t> hs(nroots);
   if (nroots) GRE_CUDA(cudaMemcpy(hs.data(), roots, sizeof(uint32_t) * nroots, cudaMemcpyDefault));
-  for (uint32_t s : hs)
-    if (s >= n) return GRE_INVALID_ARG;
-  int32_t* dl;
+  GRE_CHECK(map_ids(g, &hs, "gre_bfs_multiroot"));
+  int32_t *dfinal, *dl;
   uint32_t* droot;
-  GRE_CHECK(prepare_output(g, level, n, WS_OUTBUF, &dl));
+  GRE_CHECK(prepare_output(g, level, n, WS_OUTBUF, &dfinal));
+  GRE_CHECK(perm_out_begin(g, dfinal, 1, 4, (void**)&dl));
   GRE_CHECK(ws_array(g, WS_H, nroots ? nroots : 1, &droot));
   RunTimer timer(g);
   if (nroots) GRE_CUDA(cudaMemcpyAsync(droot, hs.data(), sizeof(uint32_t) * nroots, cudaMemcpyHostToDevice, g->stream));
   GRE_CHECK(bfs_levels(g, droot, nroots, dl, st, true));
   uint64_t e = 0;
   GRE_CHECK(count_reached_edges(g, dl, &e));
-  GRE_CHECK(finish_output(g, level, dl, n));
+  GRE_CHECK(perm_out_end(g, dl, dfinal, 1, 4));
+  GRE_CHECK(finish_output(g, level, dfinal, n));
   GRE_CHECK(timer.stop(st));
   if (st) st->traversed_edges = e;
   return GRE_SUCCESS;
@@ -440,12 +439,12 @@ int gre_msbfs(gre_graph g, const uint32_t* srcs, uint32_t nsrc, int32_t* levels,
   const uint64_t n = g->n;
   std::vector<uint32_t> hs(nsrc);
   if (nsrc) GRE_CUDA(cudaMemcpy(hs.data(), srcs, sizeof(uint32_t) * nsrc, cudaMemcpyDefault));
-  for (uint32_t s : hs)
-    if (s >= n) return GRE_INVALID_ARG;
-  int32_t* dl;
+  GRE_CHECK(map_ids(g, &hs, "gre_msbfs"));
+  int32_t *dfinal, *dl;
   unsigned long long *seen, *fa, *fb, *cnt;
   uint32_t* dsrc;
-  GRE_CHECK(prepare_output(g, levels, (uint64_t)nsrc * n, WS_OUTBUF, &dl));
+  GRE_CHECK(prepare_output(g, levels, (uint64_t)nsrc * n, WS_OUTBUF, &dfinal));
+  GRE_CHECK(perm_out_begin(g, dfinal, nsrc, 4, (void**)&dl));
   GRE_CHECK(ws_array(g, WS_A, n, &seen));
   GRE_CHECK(ws_array(g, WS_B, n, &fa));
   GRE_CHECK(ws_array(g, WS_C, n, &fb));
@@ -488,7 +487,8 @@ int gre_msbfs(gre_graph g, const uint32_t* srcs, uint32_t nsrc, int32_t* levels,
     GRE_CHECK(count_reached_edges(g, dl + (uint64_t)i * n, &e));
     edges += e;
   }
-  GRE_CHECK(finish_output(g, levels, dl, (uint64_t)nsrc * n));
+  GRE_CHECK(perm_out_end(g, dl, dfinal, nsrc, 4));
+  GRE_CHECK(finish_output(g, levels, dfinal, (uint64_t)nsrc * n));
   GRE_CHECK(timer.stop(st));
   if (st) {
     st->supersteps = max_levels;

@@ -30,13 +30,17 @@ __device__ __forceinline__ uint32_t uf_find(uint32_t* parent, uint32_t x) {
   return x;
 }
 
-__device__ __forceinline__ void uf_union(uint32_t* parent, uint32_t a, uint32_t b) {
+// key(x): the caller's vid of internal vertex x (relabelled graphs) - roots are linked by it
+__device__ __forceinline__ uint32_t uf_key(const uint32_t* __restrict__ vid, uint32_t x) { return vid ? __ldg(vid + x) : x; }
+
+__device__ __forceinline__ void uf_union(uint32_t* parent, const uint32_t* __restrict__ vid, uint32_t a, uint32_t b) {
   while (true) {
     a = uf_find(parent, a);
     b = uf_find(parent, b);
     if (a == b) return;
-    const uint32_t hi = a > b ? a : b;
-    const uint32_t lo = a > b ? b : a;
+    const bool a_hi = uf_key(vid, a) > uf_key(vid, b);
+    const uint32_t hi = a_hi ? a : b;
+    const uint32_t lo = a_hi ? b : a;
     if (atomicCAS(parent + hi, hi, lo) == hi) return;
     // hi gained a parent meanwhile: retry from the new roots
     a = hi;
@@ -47,10 +51,11 @@ __device__ __forceinline__ void uf_union(uint32_t* parent, uint32_t a, uint32_t 
 struct HookArcs {
   const uint32_t* __restrict__ col;
   uint32_t* parent;
-  bool half;  // symmetric: use only arcs with col < row
+  const uint32_t* __restrict__ vid;  // internal -> caller id, null when not relabelled
+  bool half;                          // symmetric: use only arcs with col < row
   __device__ __forceinline__ double operator()(uint32_t u, uint64_t a) const {
     const uint32_t v = __ldg(col + a);
-    if (!half || v < u) uf_union(parent, u, v);
+    if (!half || v < u) uf_union(parent, vid, u, v);
     return 0.0;
   }
 };
@@ -63,9 +68,10 @@ __global__ void k_uf_init(uint64_t n, uint32_t* __restrict__ parent) {
     parent[v] = (uint32_t)v;
 }
 
-__global__ void k_uf_flatten(uint64_t n, uint32_t* parent, uint32_t* __restrict__ label) {
+// label (in caller ids) of every internal vertex: the key of its root
+__global__ void k_uf_flatten(uint64_t n, uint32_t* parent, const uint32_t* __restrict__ vid, uint32_t* __restrict__ label) {
   for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x)
-    label[v] = uf_find(parent, (uint32_t)v);
+    label[v] = uf_key(vid, uf_find(parent, (uint32_t)v));
 }
 
 __global__ void k_count_roots(uint64_t n, const uint32_t* __restrict__ label, unsigned long long* __restrict__ c) {
@@ -88,20 +94,23 @@ int gre_cc(gre_graph g, uint32_t* label, gre_stats* st) {
   stats_reset(st);
   const uint64_t n = g->n;
   GRE_CHECK(ensure_bins(g, false));
-  uint32_t *dl, *parent;
+  uint32_t *dfinal, *dl, *parent;
   double* partial;
   void* p;
-  GRE_CHECK(prepare_output(g, label, n, WS_OUTBUF, &dl));
+  GRE_CHECK(prepare_output(g, label, n, WS_OUTBUF, &dfinal));
+  GRE_CHECK(perm_out_begin(g, dfinal, 1, 4, (void**)&dl));
   GRE_CHECK(g->ws.get(WS_A, sizeof(uint32_t) * n, &p));
   parent = (uint32_t*)p;
   GRE_CHECK(g->ws.get(WS_B, sizeof(double) * (g->bins_out.n_hub_chunks + 1), &p));
   partial = (double*)p;
   RunTimer timer(g);
   k_uf_init<<<grid_for(n, 256), 256, 0, g->stream>>>(n, parent);
-  GRE_CHECK(rows::reduce_rows(g->bins_out, g->off, HookArcs{g->col, parent, g->symmetric()}, NoFinish{}, partial, g->stream));
-  k_uf_flatten<<<grid_for(n, 256), 256, 0, g->stream>>>(n, parent, dl);
+  GRE_CHECK(rows::reduce_rows(g->bins_out, g->off, HookArcs{g->col, parent, g->perm, g->symmetric()}, NoFinish{}, partial,
+                              g->stream));
+  k_uf_flatten<<<grid_for(n, 256), 256, 0, g->stream>>>(n, parent, g->perm, dl);
   GRE_LAUNCH_CHECK();
-  GRE_CHECK(finish_output(g, label, dl, n));
+  GRE_CHECK(perm_out_end(g, dl, dfinal, 1, 4));
+  GRE_CHECK(finish_output(g, label, dfinal, n));
   GRE_CHECK(timer.stop(st));
   if (st) {
     st->supersteps = 1;

@@ -163,11 +163,46 @@ __global__ void k_low32(uint64_t m, const uint64_t* __restrict__ keys, uint32_t*
     col[i] = (uint32_t)(keys[i] & 0xffffffffull);
 }
 
+// weight of every arc from its endpoints' caller ids (perm maps internal -> caller ids)
 __global__ void k_hash_weights(uint64_t n, uint64_t m, const uint64_t* __restrict__ off, const uint32_t* __restrict__ col,
-                               uint64_t wseed, uint32_t* __restrict__ w) {
+                               const uint32_t* __restrict__ perm, uint64_t wseed, uint32_t* __restrict__ w) {
   for (uint64_t a = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; a < m; a += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t u = row_of_arc(off, n, a);
-    w[a] = rmat::weight(wseed, u, col[a]);
+    const uint32_t v = col[a];
+    w[a] = perm ? rmat::weight(wseed, perm[u], perm[v]) : rmat::weight(wseed, u, v);
+  }
+}
+
+// relabelling: sort key = complement of the degree (decreasing degree, stable in id)
+__global__ void k_reorder_keys(uint64_t n, const uint64_t* __restrict__ off, uint32_t* __restrict__ keys, uint32_t* __restrict__ ids) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t d = off[v + 1] - off[v];
+    keys[v] = 0xffffffffu - (uint32_t)(d > 0xffffffffull ? 0xffffffffull : d);
+    ids[v] = (uint32_t)v;
+  }
+}
+__global__ void k_inverse_perm(uint64_t n, const uint32_t* __restrict__ perm, uint32_t* __restrict__ iperm) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    iperm[perm[i]] = (uint32_t)i;
+}
+__global__ void k_new_degree(uint64_t n, const uint32_t* __restrict__ perm, const uint64_t* __restrict__ off, uint64_t* __restrict__ deg) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i <= n; i += (uint64_t)gridDim.x * blockDim.x)
+    deg[i] = i < n ? off[perm[i] + 1] - off[perm[i]] : 0;
+}
+// warp per new row i: copy old row perm[i], mapping neighbour ids through `map` when given
+template <class T>
+__global__ void k_move_rows(uint64_t n, const uint32_t* __restrict__ perm, const uint64_t* __restrict__ old_off,
+                            const T* __restrict__ old_data, const uint64_t* __restrict__ new_off, T* __restrict__ new_data,
+                            const uint32_t* __restrict__ map) {
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31u;
+  for (uint64_t i = warp; i < n; i += nwarps) {
+    const uint64_t o0 = old_off[perm[i]], n0 = new_off[i], len = new_off[i + 1] - n0;
+    for (uint64_t k = lane; k < len; k += 32) {
+      const T x = old_data[o0 + k];
+      new_data[n0 + k] = map ? (T)map[(uint64_t)x] : x;
+    }
   }
 }
 
@@ -271,6 +306,8 @@ static void destroy_graph(gre_graph g) {
   cudaFree(g->bc_chunks.chunk_begin);
   cudaFree(g->bc_chunks.first);
   cudaFree(g->bc_fpool);
+  cudaFree(g->perm);
+  cudaFree(g->iperm);
   g->ws.release();
   if (g->ev0) cudaEventDestroy(g->ev0);
   if (g->ev1) cudaEventDestroy(g->ev1);
@@ -369,6 +406,128 @@ static int finish_graph(gre_graph g) {
   return GRE_SUCCESS;
 }
 
+// Drops everything derived from the CSR (degrees, CSC, arc maps, bins, chunk tables).
+static void drop_derived(gre_graph g) {
+  const bool alias = (g->roff == g->off);
+  if (!alias) {
+    cudaFree(g->roff);
+    cudaFree(g->rcol);
+  }
+  g->roff = nullptr;
+  g->rcol = nullptr;
+  cudaFree(g->rarc);
+  g->rarc = nullptr;
+  cudaFree(g->rw64);
+  g->rw64 = nullptr;
+  if (g->indeg != g->outdeg) cudaFree(g->indeg);
+  cudaFree(g->outdeg);
+  g->indeg = g->outdeg = nullptr;
+  for (DegreeBins* b : {&g->bins_in, &g->bins_out}) {
+    cudaFree(b->rows);
+    cudaFree(b->hub_chunk_row);
+    cudaFree(b->hub_chunk_begin);
+    cudaFree(b->hub_chunk_first);
+    *b = DegreeBins();
+  }
+  cudaFree(g->bc_chunks.rows);
+  cudaFree(g->bc_chunks.chunk_row);
+  cudaFree(g->bc_chunks.chunk_begin);
+  cudaFree(g->bc_chunks.first);
+  g->bc_chunks = ChunkTable();
+}
+
+// Relabel by decreasing degree: new row i = old row perm[i], neighbour ids mapped through
+// iperm, arc order within a row kept; weights move with their arcs.
+static int reorder_graph(gre_graph g) {
+  if (g->perm) return GRE_SUCCESS;  // already relabelled
+  const uint64_t n = g->n, m = g->m;
+  GRE_CUDA(cudaStreamSynchronize(g->stream));
+  uint32_t *k0 = nullptr, *k1 = nullptr, *v0 = nullptr, *v1 = nullptr, *perm = nullptr, *iperm = nullptr;
+  uint64_t *deg = nullptr, *noff = nullptr;
+  uint32_t* ncol = nullptr;
+  uint32_t* nw32 = nullptr;
+  double* nw64 = nullptr;
+  auto cleanup = [&]() {
+    cudaFree(k0);
+    cudaFree(k1);
+    cudaFree(v0);
+    cudaFree(v1);
+    cudaFree(deg);
+  };
+  cudaError_t e = cudaMalloc(&k0, 4 * n);
+  if (e == cudaSuccess) e = cudaMalloc(&k1, 4 * n);
+  if (e == cudaSuccess) e = cudaMalloc(&v0, 4 * n);
+  if (e == cudaSuccess) e = cudaMalloc(&v1, 4 * n);
+  if (e == cudaSuccess) e = cudaMalloc(&iperm, 4 * n);
+  if (e == cudaSuccess) e = cudaMalloc(&deg, 8 * (n + 1));
+  if (e == cudaSuccess) e = cudaMalloc(&noff, 8 * (n + 1));
+  if (e == cudaSuccess) e = cudaMalloc(&ncol, 4 * (m ? m : 1));
+  if (e == cudaSuccess && g->w32) e = cudaMalloc(&nw32, 4 * (m ? m : 1));
+  if (e == cudaSuccess && g->w64) e = cudaMalloc(&nw64, 8 * (m ? m : 1));
+  int st = e == cudaSuccess ? GRE_SUCCESS : cuda_status(e, "cudaMalloc (reorder)", __FILE__, __LINE__);
+  if (!st) {
+    k_reorder_keys<<<grid_for(n, 256), 256, 0, g->stream>>>(n, g->off, k0, v0);
+    cub::DoubleBuffer<uint32_t> dk(k0, k1), dv(v0, v1);
+    size_t tb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, dk, dv, n, 0, 32, g->stream);
+    void* tmp = nullptr;
+    st = cub_temp(g, tb, &tmp);
+    if (!st) {
+      e = cub::DeviceRadixSort::SortPairs(tmp, tb, dk, dv, n, 0, 32, g->stream);
+      if (e != cudaSuccess) st = cuda_status(e, "SortPairs (reorder)", __FILE__, __LINE__);
+    }
+    if (!st) {
+      perm = dv.Current();
+      k_inverse_perm<<<grid_for(n, 256), 256, 0, g->stream>>>(n, perm, iperm);
+      k_new_degree<<<grid_for(n + 1, 256), 256, 0, g->stream>>>(n, perm, g->off, deg);
+      tb = 0;
+      cub::DeviceScan::ExclusiveSum(nullptr, tb, deg, noff, n + 1, g->stream);
+      st = cub_temp(g, tb, &tmp);
+    }
+    if (!st) {
+      e = cub::DeviceScan::ExclusiveSum(tmp, tb, deg, noff, n + 1, g->stream);
+      if (e != cudaSuccess) st = cuda_status(e, "ExclusiveSum (reorder)", __FILE__, __LINE__);
+    }
+    if (!st) {
+      const int grid = grid_for(n * 32, 256);
+      k_move_rows<uint32_t><<<grid, 256, 0, g->stream>>>(n, perm, g->off, g->col, noff, ncol, iperm);
+      if (nw32) k_move_rows<uint32_t><<<grid, 256, 0, g->stream>>>(n, perm, g->off, g->w32, noff, nw32, nullptr);
+      if (nw64) k_move_rows<double><<<grid, 256, 0, g->stream>>>(n, perm, g->off, g->w64, noff, nw64, nullptr);
+      e = cudaStreamSynchronize(g->stream);
+      if (e != cudaSuccess) st = cuda_status(e, "reorder", __FILE__, __LINE__);
+    }
+  }
+  if (st) {
+    cleanup();
+    cudaFree(iperm);
+    cudaFree(noff);
+    cudaFree(ncol);
+    cudaFree(nw32);
+    cudaFree(nw64);
+    return st;
+  }
+  // keep the sorted ids as perm; release the other sort buffers
+  uint32_t* keep = perm;
+  if (keep == v0) v0 = nullptr;
+  else v1 = nullptr;
+  cleanup();
+  drop_derived(g);
+  cudaFree(g->off);
+  cudaFree(g->col);
+  cudaFree(g->w32);
+  cudaFree(g->w64);
+  g->off = noff;
+  g->col = ncol;
+  g->w32 = nw32;
+  g->w64 = nw64;
+  g->perm = keep;
+  g->iperm = iperm;
+  g->h_iperm.resize(n);
+  GRE_CUDA(cudaMemcpy(g->h_iperm.data(), iperm, 4 * n, cudaMemcpyDeviceToHost));
+  g->flags |= GRE_GRAPH_REORDER;
+  return GRE_SUCCESS;
+}
+
 static int validate_csr_host(uint64_t n, uint64_t m, const uint64_t* off, const uint32_t* col) {
   if (off[0] != 0 || off[n] != m) {
     set_error("row offsets must start at 0 and end at m");
@@ -399,8 +558,24 @@ static int make_from_host_csr(uint64_t n, uint64_t m, const uint64_t* off, const
   GRE_CUDA(cudaMalloc(&g->col, sizeof(uint32_t) * (m ? m : 1)));
   GRE_CUDA(cudaMemcpyAsync(g->off, off, sizeof(uint64_t) * (n + 1), cudaMemcpyHostToDevice, g->stream));
   if (m) GRE_CUDA(cudaMemcpyAsync(g->col, col, sizeof(uint32_t) * m, cudaMemcpyHostToDevice, g->stream));
+  if (flags & GRE_GRAPH_REORDER) GRE_CHECK(reorder_graph(g));
   GRE_CHECK(finish_graph(g));
   *out = guard.release();
+  return GRE_SUCCESS;
+}
+
+// Relabel an existing graph and rebuild what depends on the CSR.
+static int reorder_existing(gre_graph g) {
+  if (g->perm) return GRE_SUCCESS;
+  GRE_CHECK(reorder_graph(g));
+  GRE_CHECK(finish_graph(g));
+  if (g->w64) {
+    GRE_CHECK(ensure_rarc(g));
+    GRE_CUDA(cudaMalloc(&g->rw64, sizeof(double) * (g->m ? g->m : 1)));
+    if (g->m) k_gather_f64<<<grid_for(g->m, 256), 256, 0, g->stream>>>(g->m, g->rarc, g->w64, g->rw64);
+    GRE_LAUNCH_CHECK();
+  }
+  GRE_CUDA(cudaStreamSynchronize(g->stream));
   return GRE_SUCCESS;
 }
 
@@ -657,6 +832,10 @@ int gre_graph_union(const gre_graph* graphs, uint32_t k, int device, gre_graph* 
   bool sym = true, all_w32 = true;
   for (uint32_t i = 0; i < k; ++i) {
     if (!graphs[i]) return GRE_NULL;
+    if (graphs[i]->perm) {
+      set_error("gre_graph_union: member %u is relabelled; build the union from unrelabelled graphs", i);
+      return GRE_INVALID_ARG;
+    }
     vertex_offset[i] = n;
     n += graphs[i]->n;
     m += graphs[i]->m;
@@ -705,10 +884,20 @@ int gre_graph_info(gre_graph g, uint64_t* n, uint64_t* m, uint32_t* flags) {
   return GRE_SUCCESS;
 }
 
+int gre_graph_reorder(gre_graph g) {
+  if (!g) return GRE_NULL;
+  GRE_CHECK(use_graph(g));
+  return reorder_existing(g);
+}
+
 int gre_graph_outdegree(gre_graph g, uint32_t* outdeg) {
   if (!g || !outdeg) return GRE_NULL;
   GRE_CHECK(use_graph(g));
-  GRE_CUDA(cudaMemcpyAsync(outdeg, g->outdeg, sizeof(uint32_t) * g->n, cudaMemcpyDefault, g->stream));
+  uint32_t* dout = nullptr;
+  GRE_CHECK(prepare_output(g, outdeg, g->n, WS_OUTBUF, &dout));
+  if (g->perm) GRE_CHECK(perm_out_end(g, g->outdeg, dout, 1, 4));
+  else GRE_CUDA(cudaMemcpyAsync(dout, g->outdeg, sizeof(uint32_t) * g->n, cudaMemcpyDeviceToDevice, g->stream));
+  GRE_CHECK(finish_output(g, outdeg, dout, g->n));
   GRE_CUDA(cudaStreamSynchronize(g->stream));
   return GRE_SUCCESS;
 }
@@ -716,17 +905,31 @@ int gre_graph_outdegree(gre_graph g, uint32_t* outdeg) {
 int gre_graph_csr(gre_graph g, uint64_t* row_off, uint32_t* col) {
   if (!g || !row_off || (g->m && !col)) return GRE_NULL;
   GRE_CHECK(use_graph(g));
+  if (g->perm) return caller_csr(g, row_off, col);
   GRE_CUDA(cudaMemcpyAsync(row_off, g->off, sizeof(uint64_t) * (g->n + 1), cudaMemcpyDefault, g->stream));
   if (g->m) GRE_CUDA(cudaMemcpyAsync(col, g->col, sizeof(uint32_t) * g->m, cudaMemcpyDefault, g->stream));
   GRE_CUDA(cudaStreamSynchronize(g->stream));
   return GRE_SUCCESS;
 }
 
+// Per-arc input in the arc order of gre_graph_csr -> device array in internal arc order.
+static int upload_arcs(gre_graph g, const void* w, size_t elem, void* dst) {
+  if (!g->m) return GRE_SUCCESS;
+  const void* src = w;
+  if (!is_device_ptr(w)) {
+    void* tmp = nullptr;
+    GRE_CHECK(g->ws.get(WS_PERM_IN, elem * g->m, &tmp));
+    GRE_CUDA(cudaMemcpyAsync(tmp, w, elem * g->m, cudaMemcpyHostToDevice, g->stream));
+    src = tmp;
+  }
+  return arcs_to_internal(g, src, dst, elem);
+}
+
 int gre_graph_set_weights_u32(gre_graph g, const uint32_t* w) {
   if (!g || (g->m && !w)) return GRE_NULL;
   GRE_CHECK(use_graph(g));
   if (!g->w32) GRE_CUDA(cudaMalloc(&g->w32, sizeof(uint32_t) * (g->m ? g->m : 1)));
-  if (g->m) GRE_CUDA(cudaMemcpyAsync(g->w32, w, sizeof(uint32_t) * g->m, cudaMemcpyDefault, g->stream));
+  GRE_CHECK(upload_arcs(g, w, 4, g->w32));
   GRE_CUDA(cudaStreamSynchronize(g->stream));
   return GRE_SUCCESS;
 }
@@ -735,7 +938,7 @@ int gre_graph_set_weights_hash(gre_graph g, uint64_t wseed) {
   if (!g) return GRE_NULL;
   GRE_CHECK(use_graph(g));
   if (!g->w32) GRE_CUDA(cudaMalloc(&g->w32, sizeof(uint32_t) * (g->m ? g->m : 1)));
-  if (g->m) k_hash_weights<<<grid_for(g->m, 256), 256, 0, g->stream>>>(g->n, g->m, g->off, g->col, wseed, g->w32);
+  if (g->m) k_hash_weights<<<grid_for(g->m, 256), 256, 0, g->stream>>>(g->n, g->m, g->off, g->col, g->perm, wseed, g->w32);
   GRE_LAUNCH_CHECK();
   GRE_CUDA(cudaStreamSynchronize(g->stream));
   return GRE_SUCCESS;
@@ -745,7 +948,7 @@ int gre_graph_set_weights_f64(gre_graph g, const double* w) {
   if (!g || (g->m && !w)) return GRE_NULL;
   GRE_CHECK(use_graph(g));
   if (!g->w64) GRE_CUDA(cudaMalloc(&g->w64, sizeof(double) * (g->m ? g->m : 1)));
-  if (g->m) GRE_CUDA(cudaMemcpyAsync(g->w64, w, sizeof(double) * g->m, cudaMemcpyDefault, g->stream));
+  GRE_CHECK(upload_arcs(g, w, 8, g->w64));
   GRE_CHECK(ensure_rarc(g));
   if (!g->rw64) GRE_CUDA(cudaMalloc(&g->rw64, sizeof(double) * (g->m ? g->m : 1)));
   if (g->m) k_gather_f64<<<grid_for(g->m, 256), 256, 0, g->stream>>>(g->m, g->rarc, g->w64, g->rw64);

@@ -46,6 +46,10 @@ enum WsSlot {
   WS_OUTBUF2,
   // betweenness state (kept apart from the slots the BFS routines use)
   WS_BC0, WS_BC1, WS_BC2, WS_BC3, WS_BC4, WS_BC5, WS_BC6, WS_BC7,
+  WS_PERM_OUT,   // results in internal order, before un-permuting (relabelled graphs)
+  WS_PERM_IN,    // inputs permuted to internal order
+  WS_PERM_IN2,
+  WS_PERM_OFF,   // caller-order row offsets
   WS_NSLOTS
 };
 
@@ -105,6 +109,12 @@ struct gre_graph_s {
   uint64_t max_outdeg = 0, max_indeg = 0;
   gre::Workspace ws;
   gre::DegreeBins bins_in, bins_out;
+  // Degree-ordered relabelling (GRE_GRAPH_REORDER / gre_graph_reorder): every internal array
+  // uses internal ids; perm[i] is the caller's id of internal vertex i (the reference's
+  // lvid2vid, DistributedGraph.hpp:57-59) and iperm its inverse.  Null when not relabelled.
+  uint32_t* perm = nullptr;
+  uint32_t* iperm = nullptr;
+  std::vector<uint32_t> h_iperm;  // host copy, to map source ids
   gre::ChunkTable bc_chunks;       // in-arc rows longer than 512 arcs (betweenness)
   uint64_t* bc_fpool = nullptr;    // per-level frontier words of the batched betweenness
   uint64_t bc_fpool_levels = 0;
@@ -214,6 +224,23 @@ int ensure_rarc(gre_graph g);
 int count_reached_edges(gre_graph g, const int32_t* level, uint64_t* edges);
 // Direction-optimising BFS levels from device roots (uses slots WS_A..WS_G, WS_COUNTERS, WS_CUB).
 int bfs_levels(gre_graph g, const uint32_t* droots, uint32_t nroots, int32_t* level, gre_stats* st, bool record);
+
+// ---------------------------------------------------------------------------------------------
+// Relabelled graphs: caller ids <-> internal ids.  All no-ops when g->perm is null.
+// ---------------------------------------------------------------------------------------------
+// Caller vertex ids (host) -> internal ids, validated against n.
+int map_ids(gre_graph g, std::vector<uint32_t>* ids, const char* what);
+// Output of `rows` x n values: returns in *internal the buffer the kernels should write (the
+// output itself when not relabelled) and later un-permutes it into `out`.
+int perm_out_begin(gre_graph g, void* out_dev, uint64_t rows, size_t elem, void** internal);
+int perm_out_end(gre_graph g, const void* internal, void* out_dev, uint64_t rows, size_t elem);
+// Input of n values in caller order -> internal order (returns the input when not relabelled).
+int perm_in(gre_graph g, const void* in_dev, size_t elem, int slot, const void** internal);
+// Per-arc arrays: caller CSR order <-> internal arc order.
+int arcs_to_internal(gre_graph g, const void* in_dev, void* out_dev, size_t elem);
+int arcs_to_caller(gre_graph g, const void* in_dev, void* out_dev, size_t elem);
+// The CSR in caller ids and caller row order (arc order within a row as stored).
+int caller_csr(gre_graph g, uint64_t* off_out, uint32_t* col_out);
 
 // ---------------------------------------------------------------------------------------------
 // Device helpers

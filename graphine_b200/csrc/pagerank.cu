@@ -417,8 +417,9 @@ int gre_pagerank(gre_graph g, int variant, double d, uint32_t iters, double* pr,
   stats_reset(st);
   GRE_CHECK(ensure_bins(g, true));
   const uint64_t n = g->n;
-  double *dpr, *c0, *c1, *partial;
-  GRE_CHECK(prepare_output(g, pr, n, WS_OUTBUF, &dpr));
+  double *dout, *dpr, *c0, *c1, *partial;
+  GRE_CHECK(prepare_output(g, pr, n, WS_OUTBUF, &dout));
+  GRE_CHECK(perm_out_begin(g, dout, 1, 8, (void**)&dpr));
   GRE_CHECK(ws_array(g, WS_A, n, &c0));
   GRE_CHECK(ws_array(g, WS_B, n, &c1));
   GRE_CHECK(ws_array(g, WS_C, g->bins_in.n_hub_chunks + 1, &partial));
@@ -434,7 +435,8 @@ int gre_pagerank(gre_graph g, int variant, double d, uint32_t iters, double* pr,
     GRE_CHECK(rows::reduce_rows(g->bins_in, g->roff, GatherContrib{g->rcol, cur}, fin, partial, g->stream));
     if (refresh) std::swap(cur, nxt);
   }
-  GRE_CHECK(finish_output(g, pr, dpr, n));
+  GRE_CHECK(perm_out_end(g, dpr, dout, 1, 8));
+  GRE_CHECK(finish_output(g, pr, dout, n));
   GRE_CHECK(timer.stop(st));
   if (st) {
     st->supersteps = iters;
@@ -455,12 +457,12 @@ int gre_ppr(gre_graph g, const uint32_t* seeds, uint32_t k, double d, uint32_t i
   const uint64_t n = g->n;
   std::vector<uint32_t> hs(k);
   GRE_CUDA(cudaMemcpy(hs.data(), seeds, sizeof(uint32_t) * k, cudaMemcpyDefault));
-  for (uint32_t s : hs)
-    if (s >= n) return GRE_INVALID_ARG;
+  GRE_CHECK(map_ids(g, &hs, "gre_ppr"));
   GRE_CHECK(ensure_bins(g, true));
   const double tele = 1.0 - d;
-  double* dout;
-  GRE_CHECK(prepare_output(g, out, (uint64_t)k * n, WS_OUTBUF, &dout));
+  double *dfinal, *dout;
+  GRE_CHECK(prepare_output(g, out, (uint64_t)k * n, WS_OUTBUF, &dfinal));
+  GRE_CHECK(perm_out_begin(g, dfinal, k, 8, (void**)&dout));
   RunTimer timer(g);
   if (!batched) {
     double *c0, *c1, *partial;
@@ -518,7 +520,8 @@ int gre_ppr(gre_graph g, const uint32_t* seeds, uint32_t k, double d, uint32_t i
       st->algo_bytes = passes * iters * (8 * (n + 1) + 4 * g->m + (uint64_t)kCols * (8 * g->m + 24 * n));
     }
   }
-  GRE_CHECK(finish_output(g, out, dout, (uint64_t)k * n));
+  GRE_CHECK(perm_out_end(g, dout, dfinal, k, 8));
+  GRE_CHECK(finish_output(g, out, dfinal, (uint64_t)k * n));
   GRE_CHECK(timer.stop(st));
   if (st) {
     st->supersteps = iters;
@@ -540,13 +543,15 @@ int gre_pagerank_weighted(gre_graph g, double d, const double* pers, double tol,
   const double* dpers;
   double *dr, *xa, *xb, *res;
   GRE_CHECK(stage_input(g, pers, n, WS_G, &dpers));
+  GRE_CHECK(perm_in(g, dpers, 8, WS_PERM_IN, (const void**)&dpers));
   GRE_CHECK(prepare_output(g, r, n, WS_OUTBUF, &dr));
   GRE_CHECK(ws_array(g, WS_A, n, &xa));
   GRE_CHECK(ws_array(g, WS_B, n, &xb));
   RunTimer timer(g);
   uint32_t done = 0;
   GRE_CHECK(affine_solve(g, g->bins_in, g->roff, g->rcol, wp.pw, dpers, 1.0 - d, 1.0 - d, d, tol, max_iters, xa, xb, &res, &done, st));
-  GRE_CUDA(cudaMemcpyAsync(dr, res, sizeof(double) * n, cudaMemcpyDeviceToDevice, g->stream));
+  if (g->perm) GRE_CHECK(perm_out_end(g, res, dr, 1, 8));
+  else GRE_CUDA(cudaMemcpyAsync(dr, res, sizeof(double) * n, cudaMemcpyDeviceToDevice, g->stream));
   GRE_CHECK(finish_output(g, r, dr, n));
   GRE_CHECK(timer.stop(st));
   if (st) {
@@ -572,10 +577,15 @@ int gre_pagerank_adjoint(gre_graph g, double d, const double* r, const double* c
   double *xa, *xb, *res, *pl, *dgw, *dlam = nullptr, *dgp = nullptr;
   GRE_CHECK(stage_input(g, r, n, WS_F, &dr));
   GRE_CHECK(stage_input(g, c, n, WS_G, &dc));
+  GRE_CHECK(perm_in(g, dr, 8, WS_PERM_IN, (const void**)&dr));
+  GRE_CHECK(perm_in(g, dc, 8, WS_PERM_IN2, (const void**)&dc));
   GRE_CHECK(ws_array(g, WS_A, n, &xa));
   GRE_CHECK(ws_array(g, WS_B, n, &xb));
   GRE_CHECK(ws_array(g, WS_C, n, &pl));
-  GRE_CHECK(prepare_output(g, grad_w, m, WS_OUTBUF, &dgw));
+  double* dgw_final;
+  GRE_CHECK(prepare_output(g, grad_w, m, WS_OUTBUF, &dgw_final));
+  dgw = dgw_final;
+  if (g->perm) GRE_CHECK(ws_array(g, WS_PERM_OUT, m, &dgw));  // internal arc order first
   if (lambda) GRE_CHECK(prepare_output(g, lambda, n, WS_D, &dlam));
   if (grad_pers) GRE_CHECK(prepare_output(g, grad_pers, n, WS_E, &dgp));
   RunTimer timer(g);
@@ -588,8 +598,18 @@ int gre_pagerank_adjoint(gre_graph g, double d, const double* r, const double* c
   GRE_CUDA(cudaMemsetAsync(pl, 0, sizeof(double) * n, g->stream));
   GRE_CHECK(rows::reduce_rows(g->bins_out, g->off, GatherWeighted{g->col, wp.p, res}, FinishStore{pl}, partial, g->stream));
   k_grad_w<<<grid_for(n * 32, 256), 256, 0, g->stream>>>(n, g->off, g->col, dr, wp.s, res, pl, d, dgw);
-  if (dgp) k_scale<<<grid_for(n, 256), 256, 0, g->stream>>>(n, res, 1.0 - d, dgp);
-  if (dlam) GRE_CUDA(cudaMemcpyAsync(dlam, res, sizeof(double) * n, cudaMemcpyDeviceToDevice, g->stream));
+  GRE_LAUNCH_CHECK();
+  if (g->perm) GRE_CHECK(arcs_to_caller(g, dgw, dgw_final, 8));
+  dgw = dgw_final;
+  if (dgp) {
+    // (1-d) lambda into pl (free now), then to caller order
+    k_scale<<<grid_for(n, 256), 256, 0, g->stream>>>(n, res, 1.0 - d, g->perm ? pl : dgp);
+    if (g->perm) GRE_CHECK(perm_out_end(g, pl, dgp, 1, 8));
+  }
+  if (dlam) {
+    if (g->perm) GRE_CHECK(perm_out_end(g, res, dlam, 1, 8));
+    else GRE_CUDA(cudaMemcpyAsync(dlam, res, sizeof(double) * n, cudaMemcpyDeviceToDevice, g->stream));
+  }
   GRE_LAUNCH_CHECK();
   GRE_CHECK(finish_output(g, grad_w, dgw, m));
   if (lambda) GRE_CHECK(finish_output(g, lambda, dlam, n));

@@ -55,10 +55,11 @@ struct VcBFS {
   unsigned long long* scat;
   unsigned long long* comb;
   int32_t* level;
-  int32_t cur = 0;  // superstep index, advanced by reduce()
+  const uint32_t* vid;  // get_vid (DistributedGraph.hpp:57-59): internal -> caller id, null = identity
+  int32_t cur = 0;      // superstep index, advanced by reduce()
   __device__ bool init(uint32_t v) {
-    pred[v] = v;
-    scat[v] = v;
+    pred[v] = vid ? vid[v] : v;  // pred[lv] = graph.get_vid(lv)
+    scat[v] = pred[v];
     if (level) level[v] = 0;
     return true;
   }
@@ -113,10 +114,11 @@ struct VcCC {
   uint32_t* cc;
   uint32_t* scat;
   uint32_t* comb;
+  const uint32_t* vid;  // get_vid: internal -> caller id, null = identity
   __device__ bool init(uint32_t v) {
-    cc[v] = v;
-    scat[v] = v;
-    comb[v] = v;
+    cc[v] = vid ? vid[v] : v;  // cc[lv] = graph.get_vid(lv)
+    scat[v] = cc[v];
+    comb[v] = cc[v];
     return true;
   }
   template <class Ctx>

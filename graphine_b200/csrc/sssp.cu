@@ -164,14 +164,11 @@ int gre_sssp(gre_graph g, const uint32_t* srcs, uint32_t nsrc, uint32_t* dist, g
   const uint64_t n = g->n;
   std::vector<uint32_t> hs(nsrc);
   if (nsrc) GRE_CUDA(cudaMemcpy(hs.data(), srcs, sizeof(uint32_t) * nsrc, cudaMemcpyDefault));
-  for (uint32_t s : hs)
-    if (s >= n) {
-      set_error("gre_sssp: source %u >= n", s);
-      return GRE_INVALID_ARG;
-    }
-  uint32_t* dd;
+  GRE_CHECK(map_ids(g, &hs, "gre_sssp"));
+  uint32_t *dfinal, *dd;
   int32_t* lv;
-  GRE_CHECK(prepare_output(g, dist, (uint64_t)nsrc * n, WS_OUTBUF, &dd));
+  GRE_CHECK(prepare_output(g, dist, (uint64_t)nsrc * n, WS_OUTBUF, &dfinal));
+  GRE_CHECK(perm_out_begin(g, dfinal, nsrc, 4, (void**)&dd));
   GRE_CHECK(ws_array(g, WS_H, n, &lv));
   RunTimer timer(g);
   uint64_t edges = 0;
@@ -182,7 +179,8 @@ int gre_sssp(gre_graph g, const uint32_t* srcs, uint32_t nsrc, uint32_t* dist, g
     GRE_CHECK(count_reached_edges(g, lv, &e));
     edges += e;
   }
-  GRE_CHECK(finish_output(g, dist, dd, (uint64_t)nsrc * n));
+  GRE_CHECK(perm_out_end(g, dd, dfinal, nsrc, 4));
+  GRE_CHECK(finish_output(g, dist, dfinal, (uint64_t)nsrc * n));
   GRE_CHECK(timer.stop(st));
   if (st) st->traversed_edges = edges;
   return GRE_SUCCESS;

@@ -54,9 +54,10 @@ int gre_vc_pagerank(gre_graph g, int variant, uint32_t max_supersteps, double* p
   GRE_CHECK(use_graph(g));
   stats_reset(st);
   const uint64_t n = g->n;
-  double *dpr, *scat, *comb;
+  double *dfinal, *dpr, *scat, *comb;
   void* scratch;
-  GRE_CHECK(prepare_output(g, pr, n, WS_OUTBUF, &dpr));
+  GRE_CHECK(prepare_output(g, pr, n, WS_OUTBUF, &dfinal));
+  GRE_CHECK(perm_out_begin(g, dfinal, 1, 8, (void**)&dpr));
   GRE_CHECK(ws_array(g, WS_B, n, &scat));
   GRE_CHECK(ws_array(g, WS_C, n, &comb));
   GRE_CHECK(g->ws.get(WS_D, vc_scratch_bytes(n), &scratch));
@@ -66,62 +67,80 @@ int gre_vc_pagerank(gre_graph g, int variant, uint32_t max_supersteps, double* p
   SourceSet all;
   all.all = true;
   GRE_CHECK(run_engine(g, vc, GRE_DIR_OUT, all, max_supersteps, scratch, st, nullptr, nullptr));
-  GRE_CHECK(finish_output(g, pr, dpr, n));
+  GRE_CHECK(perm_out_end(g, dpr, dfinal, 1, 8));
+  GRE_CHECK(finish_output(g, pr, dfinal, n));
   GRE_CHECK(timer.stop(st));
   if (st) st->traversed_edges = st->arcs_traversed;
   return GRE_SUCCESS;
 }
 
+}  // extern "C"
+
+// internal-order result -> caller output (device or host); `slot` stages host outputs
+template <class T>
+static int emit(gre_graph g, T* out, const T* internal, int slot) {
+  if (!out) return GRE_SUCCESS;
+  T* dout;
+  GRE_CHECK(prepare_output(g, out, g->n, slot, &dout));
+  if (g->perm) GRE_CHECK(perm_out_end(g, internal, dout, 1, sizeof(T)));
+  else if (dout != internal) GRE_CUDA(cudaMemcpyAsync(dout, internal, sizeof(T) * g->n, cudaMemcpyDeviceToDevice, g->stream));
+  return finish_output(g, out, dout, g->n);
+}
+
+extern "C" {
+
 int gre_vc_bfs(gre_graph g, uint32_t src, int dir, uint64_t* pred, int32_t* level, gre_stats* st) {
   if (!g) return GRE_NULL;
-  if (src >= g->n || dir < GRE_DIR_OUT || dir > GRE_DIR_INOUT) return GRE_INVALID_ARG;
+  if (dir < GRE_DIR_OUT || dir > GRE_DIR_INOUT) return GRE_INVALID_ARG;
   GRE_CHECK(use_graph(g));
+  std::vector<uint32_t> hs(1, src);
+  GRE_CHECK(map_ids(g, &hs, "gre_vc_bfs"));
   stats_reset(st);
   const uint64_t n = g->n;
-  unsigned long long *dpred = nullptr, *scat, *comb;
-  int32_t* dlevel = nullptr;
+  unsigned long long *dpred, *scat, *comb;
+  int32_t* dlevel;
   const uint32_t* dsrc;
   void* scratch;
-  if (pred) GRE_CHECK(prepare_output(g, (unsigned long long*)pred, n, WS_OUTBUF, &dpred));
-  else GRE_CHECK(ws_array(g, WS_OUTBUF, n, &dpred));
-  if (level) GRE_CHECK(prepare_output(g, level, n, WS_OUTBUF2, &dlevel));
+  GRE_CHECK(ws_array(g, WS_A, n, &dpred));
+  GRE_CHECK(ws_array(g, WS_I, n, &dlevel));
   GRE_CHECK(ws_array(g, WS_B, n, &scat));
   GRE_CHECK(ws_array(g, WS_C, n, &comb));
   GRE_CHECK(g->ws.get(WS_D, vc_scratch_bytes(n), &scratch));
   RunTimer timer(g);
-  GRE_CHECK(stage_input(g, &src, 1, WS_E, &dsrc));
+  GRE_CHECK(stage_input(g, hs.data(), 1, WS_E, &dsrc));
   GRE_CUDA(cudaMemsetAsync(dpred, 0xff, sizeof(unsigned long long) * n, g->stream));  // allocVertexData(pred, -1)
   GRE_CUDA(cudaMemsetAsync(comb, 0xff, sizeof(unsigned long long) * n, g->stream));   // allocCombineData(pred_combine, -1)
-  if (dlevel) GRE_CUDA(cudaMemsetAsync(dlevel, 0xff, sizeof(int32_t) * n, g->stream));
-  VcBFS vc{dpred, scat, comb, dlevel, 0};
+  GRE_CUDA(cudaMemsetAsync(dlevel, 0xff, sizeof(int32_t) * n, g->stream));
+  VcBFS vc{dpred, scat, comb, dlevel, g->perm, 0};
   SourceSet s;
   s.dev_vertices = dsrc;
   s.count = 1;
   GRE_CHECK(run_engine(g, vc, dir, s, 1024, scratch, st, nullptr, nullptr));
-  if (pred) GRE_CHECK(finish_output(g, (unsigned long long*)pred, dpred, n));
-  if (level) GRE_CHECK(finish_output(g, level, dlevel, n));
+  GRE_CHECK(emit(g, (unsigned long long*)pred, dpred, WS_OUTBUF));
+  GRE_CHECK(emit(g, level, dlevel, WS_OUTBUF2));
   GRE_CHECK(timer.stop(st));
   return GRE_SUCCESS;
 }
 
 int gre_vc_sssp(gre_graph g, uint32_t src, uint32_t max_supersteps, uint32_t* dist, gre_stats* st) {
   if (!g || !dist) return GRE_NULL;
-  if (src >= g->n) return GRE_INVALID_ARG;
   if (!g->w32) {
     set_error("gre_vc_sssp: the graph has no uint32 weights (gre_graph_set_weights_*)");
     return GRE_INVALID_ARG;
   }
   GRE_CHECK(use_graph(g));
+  std::vector<uint32_t> hs(1, src);
+  GRE_CHECK(map_ids(g, &hs, "gre_vc_sssp"));
   stats_reset(st);
   const uint64_t n = g->n;
   uint32_t *states, *last;
   const uint32_t* dsrc;
   void* scratch;
-  GRE_CHECK(prepare_output(g, dist, n, WS_OUTBUF, &states));
+  GRE_CHECK(ws_array(g, WS_A, n, &states));
   GRE_CHECK(ws_array(g, WS_B, n, &last));
   GRE_CHECK(g->ws.get(WS_D, vc_scratch_bytes(n), &scratch));
   RunTimer timer(g);
-  GRE_CHECK(stage_input(g, &src, 1, WS_E, &dsrc));
+  GRE_CHECK(stage_input(g, hs.data(), 1, WS_E, &dsrc));
   GRE_CUDA(cudaMemsetAsync(states, 0xff, sizeof(uint32_t) * n, g->stream));  // numeric_limits<dist_t>::max()
   GRE_CUDA(cudaMemsetAsync(last, 0, sizeof(uint32_t) * n, g->stream));
   VcSSSP vc{states, last, g->w32};
@@ -130,7 +149,7 @@ int gre_vc_sssp(gre_graph g, uint32_t src, uint32_t max_supersteps, uint32_t* di
   s.count = 1;
   uint64_t last_active = 0;
   GRE_CHECK(run_engine(g, vc, GRE_DIR_OUT, s, max_supersteps, scratch, st, nullptr, &last_active));
-  GRE_CHECK(finish_output(g, dist, states, n));
+  GRE_CHECK(emit(g, dist, states, WS_OUTBUF));
   GRE_CHECK(timer.stop(st));
   return last_active ? GRE_UNFINISHED : GRE_SUCCESS;
 }
@@ -142,18 +161,18 @@ int gre_vc_cc(gre_graph g, uint32_t* label, gre_stats* st) {
   const uint64_t n = g->n;
   uint32_t *cc, *scat, *comb;
   void* scratch;
-  GRE_CHECK(prepare_output(g, label, n, WS_OUTBUF, &cc));
+  GRE_CHECK(ws_array(g, WS_A, n, &cc));
   GRE_CHECK(ws_array(g, WS_B, n, &scat));
   GRE_CHECK(ws_array(g, WS_C, n, &comb));
   GRE_CHECK(g->ws.get(WS_D, vc_scratch_bytes(n), &scratch));
   RunTimer timer(g);
   GRE_CUDA(cudaMemsetAsync(cc, 0xff, sizeof(uint32_t) * n, g->stream));
   GRE_CUDA(cudaMemsetAsync(comb, 0xff, sizeof(uint32_t) * n, g->stream));
-  VcCC vc{cc, scat, comb};
+  VcCC vc{cc, scat, comb, g->perm};
   SourceSet all;
   all.all = true;
   GRE_CHECK(run_engine(g, vc, GRE_DIR_INOUT, all, 1024, scratch, st, nullptr, nullptr));
-  GRE_CHECK(finish_output(g, label, cc, n));
+  GRE_CHECK(emit(g, label, cc, WS_OUTBUF));
   GRE_CHECK(timer.stop(st));
   return GRE_SUCCESS;
 }
@@ -165,13 +184,12 @@ int gre_vc_bc(gre_graph g, const uint32_t* srcs, uint32_t nsrc, double* bc, gre_
   const uint64_t n = g->n;
   std::vector<uint32_t> hs(nsrc);
   if (nsrc) GRE_CUDA(cudaMemcpy(hs.data(), srcs, sizeof(uint32_t) * nsrc, cudaMemcpyDefault));
-  for (uint32_t s : hs)
-    if (s >= n) return GRE_INVALID_ARG;
+  GRE_CHECK(map_ids(g, &hs, "gre_vc_bc"));
   int32_t* level;
   double *sigma, *fscat, *fsum, *dep, *pathwgt, *bsum, *dbc;
   uint32_t* dsrc;
   void* scratch;
-  GRE_CHECK(prepare_output(g, bc, n, WS_OUTBUF, &dbc));
+  GRE_CHECK(ws_array(g, WS_J, n, &dbc));
   GRE_CHECK(ws_array(g, WS_A, n, &level));
   GRE_CHECK(ws_array(g, WS_B, n, &sigma));
   GRE_CHECK(ws_array(g, WS_C, n, &fscat));
@@ -209,7 +227,7 @@ int gre_vc_bc(gre_graph g, const uint32_t* srcs, uint32_t nsrc, double* bc, gre_
     k_bc_accumulate<<<grid_for(n, 256), 256, 0, g->stream>>>(n, s, dep, dbc);
     GRE_LAUNCH_CHECK();
   }
-  GRE_CHECK(finish_output(g, bc, dbc, n));
+  GRE_CHECK(emit(g, bc, dbc, WS_OUTBUF));
   GRE_CHECK(timer.stop(st));
   return GRE_SUCCESS;
 }

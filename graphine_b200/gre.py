@@ -34,6 +34,7 @@ GRE_INITIALIZED, GRE_UNINITIALIZED, GRE_NOT_IMPLEMENTED, GRE_INVALID_ARG = 6, 7,
 GRE_IO_ERROR, GRE_CUDA_ERROR, GRE_OOM, GRE_TIMEOUT, GRE_NO_DEVICE = 10, 11, 12, 13, 14
 Out, In, InOut = 0, 1, 2  # enum Dir (include/Types.hpp:33)
 SYMMETRIC = 0x10
+REORDER = 0x20
 PR_REFERENCE, PR_ITER = 0, 1
 MAX_RECORDED = 1024
 
@@ -107,6 +108,7 @@ def lib() -> C.CDLL:
             "gre_graph_rmat": (I32, [U32, U32, U64, I32, I32, C.POINTER(P)]),
             "gre_graph_union": (I32, [P, U32, I32, C.POINTER(P), P]),
             "gre_graph_free": (I32, [P]),
+            "gre_graph_reorder": (I32, [P]),
             "gre_graph_info": (I32, [P, C.POINTER(U64), C.POINTER(U64), C.POINTER(U32)]),
             "gre_graph_outdegree": (I32, [P, P]),
             "gre_graph_csr": (I32, [P, P, P]),
@@ -211,36 +213,50 @@ class Graph:
 
     # --- construction -------------------------------------------------------------------------
     @classmethod
-    def ingress(cls, prefix: str, dir: int = Out, symmetric: bool = False, device: int = 0) -> "Graph":
+    def ingress(cls, prefix: str, dir: int = Out, symmetric: bool = False, device: int = 0,
+                reorder: bool = False) -> "Graph":
         """DistributedGraph::ingress<dir>(comm, pool, prefix, "ascii", "edgelists")."""
         h = C.c_void_p()
-        flags = dir | (SYMMETRIC if symmetric else 0)
+        flags = dir | (SYMMETRIC if symmetric else 0) | (REORDER if reorder else 0)
         _check(lib().gre_graph_load(prefix.encode(), flags, device, C.byref(h)), "gre_graph_load")
         return cls(h.value)
 
     load = ingress
 
     @classmethod
-    def from_edges(cls, n: int, src, dst, dir: int = Out, symmetric: bool = False, device: int = 0) -> "Graph":
+    def from_edges(cls, n: int, src, dst, dir: int = Out, symmetric: bool = False, device: int = 0,
+                   reorder: bool = False) -> "Graph":
         s, d = _as(src, np.uint32), _as(dst, np.uint32)
         h = C.c_void_p()
-        _check(lib().gre_graph_from_edges(n, len(s), _ptr(s), _ptr(d), dir | (SYMMETRIC if symmetric else 0), device,
-                                          C.byref(h)), "gre_graph_from_edges")
+        flags = dir | (SYMMETRIC if symmetric else 0) | (REORDER if reorder else 0)
+        _check(lib().gre_graph_from_edges(n, len(s), _ptr(s), _ptr(d), flags, device, C.byref(h)), "gre_graph_from_edges")
         return cls(h.value)
 
     @classmethod
-    def from_csr(cls, n: int, off, col, dir: int = Out, symmetric: bool = False, device: int = 0) -> "Graph":
+    def from_csr(cls, n: int, off, col, dir: int = Out, symmetric: bool = False, device: int = 0,
+                 reorder: bool = False) -> "Graph":
         o, c = _as(off, np.uint64), _as(col, np.uint32)
         h = C.c_void_p()
-        _check(lib().gre_graph_from_csr(n, len(c), _ptr(o), _ptr(c), dir | (SYMMETRIC if symmetric else 0), device,
-                                        C.byref(h)), "gre_graph_from_csr")
+        flags = dir | (SYMMETRIC if symmetric else 0) | (REORDER if reorder else 0)
+        _check(lib().gre_graph_from_csr(n, len(c), _ptr(o), _ptr(c), flags, device, C.byref(h)), "gre_graph_from_csr")
         return cls(h.value)
 
     @classmethod
-    def rmat(cls, scale: int, edgefactor: int = 16, seed: int = 1, symmetric: bool = True, device: int = 0) -> "Graph":
+    def rmat(cls, scale: int, edgefactor: int = 16, seed: int = 1, symmetric: bool = True, device: int = 0,
+             reorder: bool = False) -> "Graph":
         h = C.c_void_p()
         _check(lib().gre_graph_rmat(scale, edgefactor, seed, int(symmetric), device, C.byref(h)), "gre_graph_rmat")
-        return cls(h.value)
+        g = cls(h.value)
+        if reorder:
+            g.reorder()
+        return g
+
+    def reorder(self) -> None:
+        """Relabel the stored graph by decreasing degree (invisible to callers)."""
+        _check(lib().gre_graph_reorder(self._h), "gre_graph_reorder")
+        n, m, f = C.c_uint64(), C.c_uint64(), C.c_uint32()
+        _check(lib().gre_graph_info(self._h, C.byref(n), C.byref(m), C.byref(f)), "gre_graph_info")
+        self.flags = f.value
 
     @classmethod
     def union(cls, graphs: Sequence["Graph"], device: int = 0):

@@ -54,7 +54,8 @@ enum gre_dir { GRE_DIR_OUT = 0, GRE_DIR_IN = 1, GRE_DIR_INOUT = 2 };
 
 /* Graph flags for the loaders (OR-ed with a direction). */
 enum gre_graph_flags {
-  GRE_GRAPH_SYMMETRIC = 0x10 /* every arc (u,v) has its reverse: the CSR doubles as CSC */
+  GRE_GRAPH_SYMMETRIC = 0x10, /* every arc (u,v) has its reverse: the CSR doubles as CSC */
+  GRE_GRAPH_REORDER = 0x20    /* store vertices by decreasing degree (gre_graph_reorder) */
 };
 
 /* PageRank variants. */
@@ -116,14 +117,22 @@ int gre_graph_rmat(uint32_t scale, uint32_t edgefactor, uint64_t seed, int symme
 int gre_graph_union(const gre_graph* graphs, uint32_t k, int device, gre_graph* out,
                     uint64_t* vertex_offset);
 int gre_graph_free(gre_graph g);
+/* Relabel the stored graph by decreasing degree (ties by id) so the state of high-degree
+ * vertices is packed together and stays cache-resident during random gathers.  Invisible to
+ * callers: every entry point keeps taking and returning caller vertex ids, caller vertex order
+ * and the arc order of gre_graph_csr.  Plays the role of the reference's local/global id maps
+ * (lvid2vid, Graph/DistributedGraph.hpp:57-59).  Graphs built with GRE_GRAPH_REORDER are
+ * relabelled on construction.  Arc weights already set are carried along. */
+int gre_graph_reorder(gre_graph g);
 /* get_num_masters / get_num_edges (DistributedGraph.hpp:93-110). */
 int gre_graph_info(gre_graph g, uint64_t* n, uint64_t* m, uint32_t* flags);
 /* getOutdegree for every vertex (DistributedGraph.hpp:178-180). */
 int gre_graph_outdegree(gre_graph g, uint32_t* outdeg);
-/* Copy the CSR back (row_off[n+1], col[m]). */
+/* Copy the CSR back (row_off[n+1], col[m]) in caller ids; its arc order is the order every
+ * per-arc array of this ABI uses (weights, gradients). */
 int gre_graph_csr(gre_graph g, uint64_t* row_off, uint32_t* col);
 /* DistributedGraph::loadEdgeProperty (DistributedGraph.hpp:195-226): uint32 weight per arc in
- * CSR order.  The CSC copy is derived on the device. */
+ * the arc order of gre_graph_csr. */
 int gre_graph_set_weights_u32(gre_graph g, const uint32_t* w);
 /* Weight of arc (u,v) = 1 + H(wseed, min(u,v), max(u,v)) % 255 (gre_sssp_weight), computed
  * on the device for every arc. */

@@ -15,11 +15,11 @@ pytestmark = pytest.mark.gpu
 D = 0.85
 
 
-def weighted_graph(scale, seed, directed=False):
+def weighted_graph(scale, seed, directed=False, reorder=False):
     n, off, col = G.rmat_host(scale, 16, seed, not directed)
     rng = np.random.default_rng(seed)
     w = np.exp(rng.standard_normal(len(col)))  # lognormal(0, 1) per arc
-    g = G.Graph.from_csr(n, off, col, dir=G.InOut if not directed else G.Out, symmetric=not directed)
+    g = G.Graph.from_csr(n, off, col, dir=G.InOut if not directed else G.Out, symmetric=not directed, reorder=reorder)
     g.set_weights_f64(w)
     return n, off, col, w, g
 
@@ -34,8 +34,9 @@ def dense_P(n, off, col, w):
     return P
 
 
-def test_weighted_forward_and_adjoint_vs_dense_solve():
-    n, off, col, w, g = weighted_graph(10, 3, directed=True)
+@pytest.mark.parametrize("reorder", [False, True], ids=["plain", "relabelled"])
+def test_weighted_forward_and_adjoint_vs_dense_solve(reorder):
+    n, off, col, w, g = weighted_graph(10, 3, directed=True, reorder=reorder)
     rng = np.random.default_rng(1)
     pers = rng.random(n) + 0.5
     c = rng.standard_normal(n)
@@ -56,8 +57,9 @@ def test_weighted_forward_and_adjoint_vs_dense_solve():
     assert rel_l1(gw, gw_ref) <= 1e-8
 
 
-def test_adjoint_vs_oracle_restatement():
-    n, off, col, w, g = weighted_graph(12, 5)
+@pytest.mark.parametrize("reorder", [False, True], ids=["plain", "relabelled"])
+def test_adjoint_vs_oracle_restatement(reorder):
+    n, off, col, w, g = weighted_graph(12, 5, reorder=reorder)
     rng = np.random.default_rng(2)
     pers = np.ones(n)
     c = rng.standard_normal(n)

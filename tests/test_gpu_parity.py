@@ -23,18 +23,23 @@ CASES = golden_cases()
 SYM = [c for c in CASES if not c.endswith("dir")]
 
 
-def graph_of(case):
+def graph_of(case, reorder=False):
     sym = bool(case["symmetric"])
-    return G.Graph.from_csr(int(case["n"]), case["off"], case["col"], dir=G.InOut if sym else G.Out, symmetric=sym)
+    return G.Graph.from_csr(int(case["n"]), case["off"], case["col"], dir=G.InOut if sym else G.Out, symmetric=sym,
+                            reorder=reorder)
+
+
+REORDER = pytest.mark.parametrize("reorder", [False, True], ids=["plain", "relabelled"])
 
 
 # ---------------------------------------------------------------------------------------------
 # golden fixtures (reference outputs)
 # ---------------------------------------------------------------------------------------------
 @pytest.mark.parametrize("name", CASES)
-def test_pagerank_golden(golden, name):
+@REORDER
+def test_pagerank_golden(golden, name, reorder):
     case = golden[name]
-    g = graph_of(case)
+    g = graph_of(case, reorder)
     pr, st = G.vc_pagerank(g, G.PR_REFERENCE, 10)
     assert rel_l1(pr, case["pr_gre10"]) <= TOL
     assert st.supersteps == 10 and st.active == list(case["pr_gre10_active"])
@@ -49,17 +54,19 @@ def test_pagerank_golden(golden, name):
 
 @pytest.mark.parametrize("name", CASES)
 @pytest.mark.parametrize("batched", [False, True])
-def test_ppr_golden(golden, name, batched):
+@REORDER
+def test_ppr_golden(golden, name, batched, reorder):
     case = golden[name]
-    g = graph_of(case)
+    g = graph_of(case, reorder)
     out, _ = G.ppr(g, case["roots"][:2], 0.85, 20, batched=batched)
     assert rel_l1(out, case["ppr20"].ravel()) <= TOL
 
 
 @pytest.mark.parametrize("name", SYM)
-def test_bfs_golden(golden, name):
+@REORDER
+def test_bfs_golden(golden, name, reorder):
     case = golden[name]
-    g = graph_of(case)
+    g = graph_of(case, reorder)
     roots = case["roots"]
     for i, r in enumerate(roots):
         pred, level, st = G.vc_bfs(g, int(r), G.In)
@@ -76,9 +83,10 @@ def test_bfs_golden(golden, name):
 
 
 @pytest.mark.parametrize("name", SYM)
-def test_sssp_golden(golden, name):
+@REORDER
+def test_sssp_golden(golden, name, reorder):
     case = golden[name]
-    g = graph_of(case)
+    g = graph_of(case, reorder)
     g.set_weights_hash(int(case["wseed"]))
     for i, r in enumerate(case["roots"]):
         dist, st, status = G.vc_sssp(g, int(r))
@@ -90,9 +98,10 @@ def test_sssp_golden(golden, name):
 
 
 @pytest.mark.parametrize("name", SYM)
-def test_cc_golden(golden, name):
+@REORDER
+def test_cc_golden(golden, name, reorder):
     case = golden[name]
-    g = graph_of(case)
+    g = graph_of(case, reorder)
     lab, st = G.vc_cc(g)
     np.testing.assert_array_equal(lab, case["cc_label"])
     assert st.active == list(case["cc_active"])
@@ -101,9 +110,10 @@ def test_cc_golden(golden, name):
 
 
 @pytest.mark.parametrize("name", SYM)
-def test_bc_golden(golden, name):
+@REORDER
+def test_bc_golden(golden, name, reorder):
     case = golden[name]
-    g = graph_of(case)
+    g = graph_of(case, reorder)
     b, _ = G.vc_bc(g, case["roots"])
     assert rel_l1(b, case["bc"]) <= TOL
     b1, _ = G.bc(g, case["roots"], batched=False)
@@ -131,10 +141,14 @@ def test_loader_matches_fixture(golden, name):
 # ---------------------------------------------------------------------------------------------
 # seeded RMAT vs the restatement
 # ---------------------------------------------------------------------------------------------
-@pytest.fixture(scope="module")
-def rmat14():
+@pytest.fixture(scope="module", params=[False, True], ids=["plain", "relabelled"])
+def rmat14(request):
     n, off, col = G.rmat_host(14, 16, 42, True)
-    g = G.Graph.from_csr(n, off, col, dir=G.InOut, symmetric=True)
+    g = G.Graph.from_csr(n, off, col, dir=G.InOut, symmetric=True, reorder=request.param)
+    if request.param:
+        o2, c2 = g.csr()  # caller ids and caller arc order survive the relabelling
+        np.testing.assert_array_equal(o2, off)
+        np.testing.assert_array_equal(c2, col)
     R = O.Restatement.from_csr(n, off, col)
     roots = G.sample_sources(off, 16, 9)
     return n, off, col, g, R, roots
@@ -287,7 +301,7 @@ def test_graph_union_batch():
 # ---------------------------------------------------------------------------------------------
 @pytest.fixture(scope="module")
 def rmat20():
-    g = G.Graph.rmat(20, 16, 2024, True)
+    g = G.Graph.rmat(20, 16, 2024, True, reorder=True)
     off, col = g.csr()
     src = np.repeat(np.arange(g.n, dtype=np.int64), np.diff(off.astype(np.int64)))
     return g, off, col, src
