@@ -224,13 +224,15 @@ __global__ void k_bin_of(uint64_t n, const uint64_t* __restrict__ off, uint8_t* 
   for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t d = off[v + 1] - off[v];
     uint8_t b;
+    // lanes per row = degree / 4 rounded up to a power of two (each lane gathers 4 arcs per
+    // pass), a CTA beyond 4096 arcs, CTA chunks beyond 65536
     if (d == 0) b = 255;
-    else if (d == 1) b = 0;
-    else if (d == 2) b = 1;
-    else if (d <= 4) b = 2;
-    else if (d <= 8) b = 3;
-    else if (d <= 16) b = 4;
-    else if (d <= 1024) b = 5;
+    else if (d <= 4) b = 0;
+    else if (d <= 8) b = 1;
+    else if (d <= 16) b = 2;
+    else if (d <= 32) b = 3;
+    else if (d <= 64) b = 4;
+    else if (d <= 4096) b = 5;
     else if (d <= 65536) b = 6;
     else b = 7;
     bin[v] = b;

@@ -27,7 +27,8 @@ namespace gre {
 struct GatherContrib {
   const uint32_t* __restrict__ rcol;
   const double* __restrict__ contrib;
-  __device__ __forceinline__ double operator()(uint32_t, uint64_t a) const { return contrib[__ldg(rcol + a)]; }
+  // contrib is read-only during a superstep (the next values go to the other buffer)
+  __device__ __forceinline__ double operator()(uint32_t, uint64_t a) const { return __ldg(contrib + __ldg(rcol + a)); }
 };
 
 struct FinishPR {
@@ -101,10 +102,28 @@ struct PprRow {
   const uint64_t* __restrict__ roff;
   const uint32_t* __restrict__ rcol;
   const double* __restrict__ contrib;
-  // adds contrib rows of arcs [a0, a1) into acc (each lane its 4 columns)
+  // adds contrib rows of arcs [a0, a1) into acc (each lane its 4 columns); two arcs per pass
+  // keep eight independent loads per lane in flight
   __device__ __forceinline__ void accumulate(uint64_t a0, uint64_t a1, double acc[kCols / 32]) const {
     const uint32_t lane = threadIdx.x & 31u;
-    for (uint64_t a = a0; a < a1; ++a) {
+    uint64_t a = a0;
+    for (; a + 1 < a1; a += 2) {
+      const uint32_t u0 = __ldg(rcol + a), u1 = __ldg(rcol + a + 1);
+      const double* r0 = contrib + (uint64_t)u0 * kCols + lane;
+      const double* r1 = contrib + (uint64_t)u1 * kCols + lane;
+      double x0[kCols / 32], x1[kCols / 32];
+#pragma unroll
+      for (int j = 0; j < kCols / 32; ++j) {
+        x0[j] = __ldg(r0 + 32 * j);
+        x1[j] = __ldg(r1 + 32 * j);
+      }
+#pragma unroll
+      for (int j = 0; j < kCols / 32; ++j) {
+        acc[j] += x0[j];
+        acc[j] += x1[j];
+      }
+    }
+    for (; a < a1; ++a) {
       const uint32_t u = __ldg(rcol + a);
       const double* row = contrib + (uint64_t)u * kCols + lane;
 #pragma unroll
@@ -134,7 +153,7 @@ struct PprFinish {
   }
 };
 
-// rows of bins 0..5 (degree <= 1024): one warp per row
+// rows of bins 0..4 (degree <= 64): one warp per row
 __global__ void __launch_bounds__(256) k_ppr_rows(const uint32_t* __restrict__ rows, uint64_t count, PprRow R, PprFinish F) {
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -199,8 +218,8 @@ struct PprChunks {
 
 static int ppr_chunks(gre_graph g, PprChunks* pc) {
   const DegreeBins& B = g->bins_in;
-  pc->nrows = B.count[6] + B.count[7];
-  pc->rows = B.rows + B.start[6];
+  pc->nrows = B.count[5] + B.count[6] + B.count[7];  // rows longer than 64 arcs
+  pc->rows = B.rows + B.start[5];
   if (!pc->nrows) return GRE_SUCCESS;
   std::vector<uint32_t> rows(pc->nrows);
   std::vector<uint64_t> ho(g->n + 1);
@@ -493,7 +512,7 @@ int gre_ppr(gre_graph g, const uint32_t* seeds, uint32_t k, double d, uint32_t i
     GRE_CHECK(ws_array(g, WS_E, kCols, &dseeds));
     const DegreeBins& B = g->bins_in;
     uint64_t short_rows = 0;
-    for (int b = 0; b < 6; ++b) short_rows += B.count[b];
+    for (int b = 0; b < 5; ++b) short_rows += B.count[b];
     for (uint32_t j0 = 0; j0 < k; j0 += kCols) {
       const uint32_t kk = (k - j0) < (uint32_t)kCols ? (k - j0) : (uint32_t)kCols;
       GRE_CUDA(cudaMemcpyAsync(dseeds, hs.data() + j0, sizeof(uint32_t) * kk, cudaMemcpyHostToDevice, g->stream));

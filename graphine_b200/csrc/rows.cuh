@@ -2,10 +2,11 @@
 // scatter+combine for sums (PageRank, weighted PageRank, its adjoint).
 //
 // Rows are grouped once per graph by degree (DegreeBins): bins 0..5 give a row 1, 2, 4, 8, 16
-// or 32 lanes (degree 1, 2, 3-4, 5-8, 9-16, 17-1024); bin 6 gives a row one CTA (1025-65536);
-// bin 7 splits a row into chunks of 65536 arcs, one CTA each, whose partial sums are added in
-// chunk order by a second kernel.  Lane j of a group adds arcs j, j+L, j+2L, ... and the group
-// reduces with xor shuffles, so every row's sum has a fixed association order: results are
+// or 32 lanes (degree 1-4, 5-8, 9-16, 17-32, 33-64, 65-4096: about four arcs per lane per
+// pass); bin 6 gives a row one CTA (4097-65536); bin 7 splits a row into chunks of 65536 arcs,
+// one CTA each, whose partial sums are added in chunk order by a second kernel.  Lane j of a
+// group adds arcs j, j+L, j+2L, ... (four independent loads per pass) and the group reduces
+// with xor shuffles, so every row's sum has a fixed association order: results are
 // deterministic run to run.  Column indices of one group are contiguous (coalesced); the
 // gathered value is the only random access.
 //
@@ -19,6 +20,24 @@ namespace rows {
 
 constexpr int kCta = 256;
 constexpr uint64_t kHubChunk = 65536;
+
+// Sum of gat(v, a) over a = a0 + lig, a0 + lig + L, ... < a1.  Four arcs per pass so that each
+// lane has four independent (column, gathered value) load chains in flight: the loop is bound
+// by memory latency, not bandwidth, when a lane waits on one chain at a time.
+template <int L, class Gather>
+__device__ __forceinline__ double strided_sum(Gather& gat, uint32_t v, uint64_t a0, uint64_t a1, uint32_t lig) {
+  double acc = 0.0;
+  uint64_t a = a0 + lig;
+  for (; a + 3 * (uint64_t)L < a1; a += 4 * (uint64_t)L) {
+    const double x0 = gat(v, a), x1 = gat(v, a + L), x2 = gat(v, a + 2 * L), x3 = gat(v, a + 3 * L);
+    acc += x0;
+    acc += x1;
+    acc += x2;
+    acc += x3;
+  }
+  for (; a < a1; a += L) acc += gat(v, a);
+  return acc;
+}
 
 template <int L, class Gather, class Finish>
 __global__ void __launch_bounds__(256) k_rows_lanes(const uint32_t* __restrict__ rows, uint64_t count,
@@ -36,8 +55,7 @@ __global__ void __launch_bounds__(256) k_rows_lanes(const uint32_t* __restrict__
     uint32_t v = 0;
     if (valid) {
       v = rows[i];
-      const uint64_t a1 = off[v + 1];
-      for (uint64_t a = off[v] + lig; a < a1; a += L) acc += gat(v, a);
+      acc = strided_sum<L>(gat, v, off[v], off[v + 1], lig);
     }
 #pragma unroll
     for (int o = L / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -65,9 +83,7 @@ __global__ void __launch_bounds__(kCta) k_rows_cta(const uint32_t* __restrict__ 
   __shared__ double smem[kCta / 32];
   for (uint64_t i = blockIdx.x; i < count; i += gridDim.x) {
     const uint32_t v = rows[i];
-    const uint64_t a1 = off[v + 1];
-    double acc = 0.0;
-    for (uint64_t a = off[v] + threadIdx.x; a < a1; a += kCta) acc += gat(v, a);
+    double acc = strided_sum<kCta>(gat, v, off[v], off[v + 1], threadIdx.x);
     acc = block_sum(acc, smem);
     if (threadIdx.x == 0) fin(v, acc);
   }
@@ -83,8 +99,7 @@ __global__ void __launch_bounds__(kCta) k_rows_chunks(const uint32_t* __restrict
     const uint64_t a0 = chunk_begin[c];
     const uint64_t end = off[v + 1];
     const uint64_t a1 = (a0 + kHubChunk < end) ? a0 + kHubChunk : end;
-    double acc = 0.0;
-    for (uint64_t a = a0 + threadIdx.x; a < a1; a += kCta) acc += gat(v, a);
+    double acc = strided_sum<kCta>(gat, v, a0, a1, threadIdx.x);
     acc = block_sum(acc, smem);
     if (threadIdx.x == 0) partial[c] = acc;
   }

@@ -1,0 +1,105 @@
+// gre_run — drop-in for the reference example drivers (usr/test_pagerank.cpp, test_bfs.cpp,
+// test_sssp.cpp, test_cc.cpp, test_bc.cpp) on libgre_gpu.so, written against gre/gre.hpp.
+//
+//   gre_run <pagerank|pagerank_iter|bfs|sssp|cc|bc> <prefix> [ascii] [edgelists]
+//
+// Same inputs (<prefix>.meta, <prefix>.edges.<i>, <prefix>.roots, source = the first root as
+// the reference's src[1]) and the same per-superstep lines the reference engine prints
+// ("Superstep-k: Number of active vertices...N", Engine.hpp:396-398), then the iteration
+// count and the run time.  Differences: one GPU, no MPI; SSSP weights come from the seeded
+// weight function (environment GRE_WSEED, default 1) instead of unseeded rand(); BC runs all
+// roots of the file and accumulates them.  Exit status 0 on success, the gre status otherwise.
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/gre/gre.hpp"
+
+static void print_supersteps(const gre_stats& st) {
+  for (uint32_t i = 0; i < st.n_recorded; ++i)
+    printf("Superstep-%u: Number of active vertices...%llu\n", i, (unsigned long long)st.active[i]);
+}
+
+int main(int argc, char** argv) {
+  if (argc < 3) {
+    fprintf(stderr, "usage: %s pagerank|pagerank_iter|bfs|sssp|cc|bc prefix [ascii] [edgelists]\n", argv[0]);
+    return 2;
+  }
+  const std::string algo(argv[1]), prefix(argv[2]);
+  try {
+    gre::DistributedGraph g;
+    const bool in_out = algo == "bfs" || algo == "cc" || algo == "bc";
+    if (in_out) g.ingress<gre::InOut>(prefix);
+    else g.ingress<gre::Out>(prefix);
+    std::vector<uint32_t> roots(1024);
+    uint32_t nroots = 0;
+    if (algo == "bfs" || algo == "sssp" || algo == "bc") {
+      int s = gre_read_roots(prefix.c_str(), roots.data(), (uint32_t)roots.size(), &nroots);
+      if ((s != GRE_SUCCESS && s != GRE_NOBUFFER) || nroots == 0) {
+        fprintf(stderr, "Err in reading src vertex from file.\n");
+        return s ? s : GRE_IO_ERROR;
+      }
+      roots.resize(nroots < roots.size() ? nroots : roots.size());
+    }
+    gre::SourceVertexSet src;
+    gre_stats st{};
+    if (algo == "pagerank" || algo == "pagerank_iter") {
+      src.setALL();
+      gre::PageRank pr(g, algo == "pagerank_iter");
+      gre::SynchronousEngine<gre::PageRank> engine(g, pr);
+      engine.initialize();
+      engine.configMaxSupersteps(algo == "pagerank" ? 10 : 20);  // usr/test_pagerank.cpp:70
+      engine.run<gre::Out>(src);
+      st = engine.stats();
+      double sum = 0;
+      for (double x : pr.pr) sum += x;
+      print_supersteps(st);
+      printf("Sum of pr: %.15g\n", sum);
+    } else if (algo == "bfs") {
+      src.addVertex(roots[0], g);
+      gre::BFS bfs(g);
+      gre::SynchronousEngine<gre::BFS> engine(g, bfs);
+      engine.run<gre::In>(src);  // usr/test_bfs.cpp:69
+      st = engine.stats();
+      print_supersteps(st);
+    } else if (algo == "sssp") {
+      const char* ws = getenv("GRE_WSEED");
+      g.loadEdgePropertyHash(ws ? strtoull(ws, nullptr, 10) : 1);
+      src.addVertex(roots[0], g);
+      gre::SSSP sssp(g);
+      gre::SynchronousEngine<gre::SSSP> engine(g, sssp);
+      engine.configMaxSupersteps(128);  // usr/test_sssp.cpp:64
+      engine.run<gre::Out>(src);
+      st = engine.stats();
+      print_supersteps(st);
+    } else if (algo == "cc") {
+      src.setALL();
+      gre::ConnectedComponents cc(g);
+      gre::SynchronousEngine<gre::ConnectedComponents> engine(g, cc);
+      engine.run<gre::InOut>(src);
+      st = engine.stats();
+      print_supersteps(st);
+      long comps = 0;
+      for (size_t v = 0; v < cc.cc.size(); ++v) comps += cc.cc[v] == v;
+      printf("Number of components: %ld\n", comps);
+    } else if (algo == "bc") {
+      for (uint32_t r : roots) src.addVertex(r, g);
+      gre::BC bc(g);
+      gre::SynchronousEngine<gre::BC> engine(g, bc);
+      engine.run<gre::Out>(src);
+      st = engine.stats();
+    } else {
+      fprintf(stderr, "unknown algorithm %s\n", algo.c_str());
+      return 2;
+    }
+    printf("B200 | Iteration count: %u\n", st.supersteps);
+    printf("B200 | Use time: %gs\n", st.device_ms * 1e-3);
+  } catch (const gre::Error& e) {
+    fprintf(stderr, "%s\n", e.what());
+    return e.status;
+  }
+  return 0;
+}

@@ -1,0 +1,168 @@
+// gre/gre.hpp — C++ host mirror of the reference GRE driver API over the C ABI (gre_gpu.h).
+//
+// The reference drivers (usr/test_*.cpp) use:
+//   DistributedGraph_t g; g.ingress<InOut>(comm, pool, prefix, format, method);
+//   SourceVertexSet srcSet; srcSet.addVertex(v, g) | srcSet.setALL();
+//   Plugin p(g); SynchronousEngine<Plugin> engine(g, comm, pool, p);
+//   engine.initialize(); engine.configMaxSupersteps(n); engine.run<Dir>(srcSet);
+//   engine.getSuperstepCount(); engine.finalize();
+// (Graph/DistributedGraph.hpp:153-172, Graph/VertexSet.hpp:286-347, Engine/Engine.hpp:94-202).
+// This header keeps those names for the five reference plugins.  The communicator and buffer
+// pool disappear (one GPU, no MPI); errors are reported as gre::Error exceptions carrying the
+// status code instead of exit(-1).  Results are read from the plugin objects after run().
+#pragma once
+#include <stdint.h>
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../gre_gpu.h"
+
+namespace gre {
+
+struct Error : std::runtime_error {
+  int status;
+  Error(int s, const std::string& where)
+      : std::runtime_error(where + ": " + gre_status_str(s) + " (" + gre_last_error() + ")"), status(s) {}
+};
+
+inline void check(int s, const char* where) {
+  if (s != GRE_SUCCESS && s != GRE_UNFINISHED) throw Error(s, where);
+}
+
+enum Dir { Out = GRE_DIR_OUT, In = GRE_DIR_IN, InOut = GRE_DIR_INOUT };
+
+// DistributedGraph<GraphInCSR> of one rank: every vertex is a master.
+class DistributedGraph {
+ public:
+  DistributedGraph() = default;
+  DistributedGraph(const DistributedGraph&) = delete;
+  DistributedGraph& operator=(const DistributedGraph&) = delete;
+  ~DistributedGraph() {
+    if (g_) gre_graph_free(g_);
+  }
+  // ingress<dir>(comm, pool, prefix, "ascii", "edgelists"); `symmetric` lets the CSR serve as
+  // CSC, `reorder` stores vertices by decreasing degree (invisible to callers).
+  template <Dir dir>
+  bool ingress(const std::string& prefix, const std::string& format = "ascii", const std::string& method = "edgelists",
+               bool symmetric = false, bool reorder = false, int device = 0) {
+    if (format != "ascii" || method != "edgelists") throw Error(GRE_NOT_IMPLEMENTED, "ingress: only ascii edgelists");
+    if (g_) gre_graph_free(g_);
+    g_ = nullptr;
+    uint32_t flags = (uint32_t)dir | (symmetric ? GRE_GRAPH_SYMMETRIC : 0u) | (reorder ? GRE_GRAPH_REORDER : 0u);
+    check(gre_graph_load(prefix.c_str(), flags, device, &g_), "gre_graph_load");
+    return true;
+  }
+  size_t get_num_masters() const { return info().first; }
+  size_t get_num_edges() const { return info().second; }
+  std::vector<uint32_t> getOutdegrees() const {
+    std::vector<uint32_t> d(get_num_masters());
+    check(gre_graph_outdegree(g_, d.data()), "gre_graph_outdegree");
+    return d;
+  }
+  // loadEdgeProperty (DistributedGraph.hpp:195-226): weights in the arc order of the CSR
+  void loadEdgeProperty(const std::vector<uint32_t>& w) { check(gre_graph_set_weights_u32(g_, w.data()), "set_weights"); }
+  void loadEdgePropertyHash(uint64_t wseed) { check(gre_graph_set_weights_hash(g_, wseed), "set_weights_hash"); }
+  gre_graph handle() const { return g_; }
+
+ private:
+  std::pair<size_t, size_t> info() const {
+    uint64_t n = 0, m = 0;
+    check(gre_graph_info(g_, &n, &m, nullptr), "gre_graph_info");
+    return {n, m};
+  }
+  gre_graph g_ = nullptr;
+};
+
+// SourceVertexSet (Graph/VertexSet.hpp:286-347)
+struct SourceVertexSet {
+  bool complete = false;
+  std::vector<uint32_t> vertices;
+  void setALL() { complete = true; }
+  bool isALL() const { return complete; }
+  void addVertex(uint64_t v, const DistributedGraph&) { vertices.push_back((uint32_t)v); }
+  void clear() {
+    complete = false;
+    vertices.clear();
+  }
+};
+
+// The reference plugins; each keeps its result arrays after the engine ran.
+struct PageRank {
+  explicit PageRank(DistributedGraph& g, bool iterate = false) : graph(g), iter(iterate) {}
+  DistributedGraph& graph;
+  bool iter;  // false: Kernels/PageRank.hpp verbatim; true: power iteration (pr_scatter refreshed)
+  std::vector<double> pr;
+};
+struct BFS {
+  explicit BFS(DistributedGraph& g) : graph(g) {}
+  DistributedGraph& graph;
+  std::vector<uint64_t> pred;  // source vid on reached vertices (the plugin forwards pred)
+  std::vector<int32_t> level;
+};
+struct SSSP {
+  explicit SSSP(DistributedGraph& g) : graph(g) {}
+  DistributedGraph& graph;
+  std::vector<uint32_t> states;  // distances
+};
+struct ConnectedComponents {
+  explicit ConnectedComponents(DistributedGraph& g) : graph(g) {}
+  DistributedGraph& graph;
+  std::vector<uint32_t> cc;  // minimum vid of the component
+};
+struct BC {  // usr/test_bc.cpp's Forward + Backward, accumulated over the sources
+  explicit BC(DistributedGraph& g) : graph(g) {}
+  DistributedGraph& graph;
+  std::vector<double> bc;
+};
+
+// SynchronousEngine<VertexCode> (Engine/Engine.hpp:54-1418) for the plugins above.
+template <class VC>
+class SynchronousEngine {
+ public:
+  SynchronousEngine(DistributedGraph& g, VC& vc) : g_(g), vc_(vc) {}
+  void initialize() {}
+  void finalize() {}
+  void configMaxSupersteps(long n) { max_ = n > 0 ? (uint32_t)n : 1024; }
+  long getSuperstepCount() const { return st_.supersteps; }
+  const gre_stats& stats() const { return st_; }
+  template <Dir dir = Out>
+  void run(const SourceVertexSet& src) {
+    runImpl(dir, src, vc_);
+  }
+
+ private:
+  const uint32_t* first(const SourceVertexSet& s) const {
+    if (s.vertices.empty()) throw Error(GRE_INVALID_ARG, "run: no source vertex");
+    return s.vertices.data();
+  }
+  void runImpl(Dir, const SourceVertexSet&, PageRank& p) {
+    p.pr.resize(g_.get_num_masters());
+    check(gre_vc_pagerank(g_.handle(), p.iter ? GRE_PR_ITER : GRE_PR_REFERENCE, max_, p.pr.data(), &st_), "gre_vc_pagerank");
+  }
+  void runImpl(Dir dir, const SourceVertexSet& s, BFS& b) {
+    b.pred.resize(g_.get_num_masters());
+    b.level.resize(g_.get_num_masters());
+    check(gre_vc_bfs(g_.handle(), *first(s), (int)dir, b.pred.data(), b.level.data(), &st_), "gre_vc_bfs");
+  }
+  void runImpl(Dir, const SourceVertexSet& s, SSSP& p) {
+    p.states.resize(g_.get_num_masters());
+    check(gre_vc_sssp(g_.handle(), *first(s), max_, p.states.data(), &st_), "gre_vc_sssp");
+  }
+  void runImpl(Dir, const SourceVertexSet&, ConnectedComponents& c) {
+    c.cc.resize(g_.get_num_masters());
+    check(gre_vc_cc(g_.handle(), c.cc.data(), &st_), "gre_vc_cc");
+  }
+  void runImpl(Dir, const SourceVertexSet& s, BC& b) {
+    b.bc.resize(g_.get_num_masters());
+    check(gre_vc_bc(g_.handle(), s.vertices.data(), (uint32_t)s.vertices.size(), b.bc.data(), &st_), "gre_vc_bc");
+  }
+
+  DistributedGraph& g_;
+  VC& vc_;
+  uint32_t max_ = 1024;
+  gre_stats st_{};
+};
+
+}  // namespace gre
