@@ -122,6 +122,7 @@ def lib() -> C.CDLL:
             "gre_vc_bc": (I32, [P, P, U32, P, S]),
             "gre_pagerank": (I32, [P, I32, D, U32, P, S]),
             "gre_bfs": (I32, [P, P, U32, P, S]),
+            "gre_bfs_noalloc": (I32, [P, U32, P, S]),
             "gre_msbfs": (I32, [P, P, U32, P, S]),
             "gre_bfs_multiroot": (I32, [P, P, U32, P, S]),
             "gre_sssp": (I32, [P, P, U32, P, S]),

@@ -172,6 +172,15 @@ int gre_vc_bc(gre_graph g, const uint32_t* srcs, uint32_t nsrc, double* bc, gre_
 int gre_pagerank(gre_graph g, int variant, double d, uint32_t iters, double* pr, gre_stats* st);
 /* Direction-optimising BFS, one run per source.  levels: nsrc x n int32 (-1 unreached). */
 int gre_bfs(gre_graph g, const uint32_t* srcs, uint32_t nsrc, int32_t* levels, gre_stats* st);
+/* No counterpart in the reference.  gre_bfs for callers that cannot let the library allocate
+ * device memory (a process whose device memory is reserved and capped by its own pool
+ * allocator, or a latency-critical loop that cannot take cudaMalloc's implicit device
+ * synchronisation): one source, `level` must be device memory (n int32), and all scratch lives
+ * in a fixed 32 MiB array inside the library, so graphs are limited to 1,048,576 vertices
+ * (larger ones: GRE_INVALID_ARG).  The array is shared by all calls on a device: calls that
+ * overlap on the GPU race.  The first call on a device looks up the array's address; make it
+ * before any stream capture. */
+int gre_bfs_noalloc(gre_graph g, uint32_t src, int32_t* level, gre_stats* st);
 /* Multi-source BFS with 64 sources per uint64 frontier word.  levels: nsrc x n int32. */
 int gre_msbfs(gre_graph g, const uint32_t* srcs, uint32_t nsrc, int32_t* levels, gre_stats* st);
 /* One BFS whose level-0 frontier holds all `nroots` roots (distance to the nearest root);
