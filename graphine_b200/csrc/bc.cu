@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "gre_internal.cuh"
+#include "msbfs.cuh"
 
 namespace gre {
 
@@ -302,19 +303,41 @@ struct BcM {
   const unsigned long long* __restrict__ fd;     // F_d
   double* sigma;                                 // [n][64]
   double* dep;                                   // [n][64]
-  // arcs [a0, a1) of vertex v; lane owns sources lane and lane+32
+  // Arcs [a0, a1) of vertex v; lane owns sources lane and lane+32.  32 arcs at a time are staged
+  // with lane = arc (column and source mask loaded 32-wide), compacted to the arcs whose mask
+  // meets v's, then walked in arc order with lane = source: the same association order as one
+  // source at a time, with the index and mask loads off the per-arc critical path.
+  // su / sm: this warp's 32-entry shared-memory staging area.
   template <bool FWD>
-  __device__ __forceinline__ void sum(uint32_t v, uint64_t a0, uint64_t a1, double& acc0, double& acc1) const {
+  __device__ __forceinline__ void sum(uint32_t v, uint64_t a0, uint64_t a1, double& acc0, double& acc1, uint32_t* su,
+                                      unsigned long long* sm) const {
     const uint32_t lane = threadIdx.x & 31u;
     const unsigned long long mine = fd[v];
-    for (uint64_t a = a0; a < a1; ++a) {
-      const uint32_t u = __ldg(rcol + a);
-      const unsigned long long m = fprev[u] & mine;
-      if (!m) continue;  // uniform across the warp
-      const uint64_t row = (uint64_t)u * 64;
-      if ((m >> lane) & 1ull) acc0 = add(acc0, FWD ? sigma[row + lane] : dep_term(dep[row + lane], sigma[row + lane]));
-      if ((m >> (lane + 32)) & 1ull)
-        acc1 = add(acc1, FWD ? sigma[row + lane + 32] : dep_term(dep[row + lane + 32], sigma[row + lane + 32]));
+    for (uint64_t base = a0; base < a1; base += 32) {
+      const uint64_t a = base + lane;
+      uint32_t u = 0;
+      unsigned long long m = 0;
+      if (a < a1) {
+        u = __ldg(rcol + a);
+        m = fprev[u] & mine;
+      }
+      const uint32_t ball = __ballot_sync(0xffffffffu, m != 0ull);
+      if (m) {
+        const uint32_t pos = __popc(ball & ((1u << lane) - 1u));
+        su[pos] = u;
+        sm[pos] = m;
+      }
+      __syncwarp();
+      const int cnt = __popc(ball);
+#pragma unroll 4
+      for (int i = 0; i < cnt; ++i) {
+        const uint64_t row = (uint64_t)su[i] * 64;
+        const unsigned long long mm = sm[i];
+        if ((mm >> lane) & 1ull) acc0 = add(acc0, FWD ? sigma[row + lane] : dep_term(dep[row + lane], sigma[row + lane]));
+        if ((mm >> (lane + 32)) & 1ull)
+          acc1 = add(acc1, FWD ? sigma[row + lane + 32] : dep_term(dep[row + lane + 32], sigma[row + lane + 32]));
+      }
+      __syncwarp();
     }
   }
   template <bool FWD>
@@ -336,6 +359,8 @@ struct BcM {
 template <bool FWD>
 __global__ void __launch_bounds__(256) k_bcm_rows(const uint32_t* __restrict__ list, const unsigned int* __restrict__ count, BcM B,
                                                   uint64_t ch) {
+  __shared__ uint32_t s_u[8][32];
+  __shared__ unsigned long long s_m[8][32];
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const uint64_t cnt = *count;
@@ -344,13 +369,15 @@ __global__ void __launch_bounds__(256) k_bcm_rows(const uint32_t* __restrict__ l
     const uint64_t a0 = B.roff[v], a1 = B.roff[v + 1];
     if (a1 - a0 > ch) continue;
     double acc0 = 0.0, acc1 = 0.0;
-    B.template sum<FWD>(v, a0, a1, acc0, acc1);
+    B.template sum<FWD>(v, a0, a1, acc0, acc1, s_u[threadIdx.x >> 5], s_m[threadIdx.x >> 5]);
     B.template store<FWD>(v, acc0, acc1);
   }
 }
 
 template <bool FWD>
 __global__ void __launch_bounds__(256) k_bcm_chunks(ChunkTable T, BcM B, double* __restrict__ partial) {
+  __shared__ uint32_t s_u[8][32];
+  __shared__ unsigned long long s_m[8][32];
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const uint32_t lane = threadIdx.x & 31u;
@@ -361,7 +388,7 @@ __global__ void __launch_bounds__(256) k_bcm_chunks(ChunkTable T, BcM B, double*
     const uint64_t end = B.roff[v + 1];
     const uint64_t a1 = a0 + T.ch < end ? a0 + T.ch : end;
     double acc0 = 0.0, acc1 = 0.0;
-    B.template sum<FWD>(v, a0, a1, acc0, acc1);
+    B.template sum<FWD>(v, a0, a1, acc0, acc1, s_u[threadIdx.x >> 5], s_m[threadIdx.x >> 5]);
     partial[c * 64 + lane] = acc0;
     partial[c * 64 + lane + 32] = acc1;
   }
@@ -414,13 +441,16 @@ static int bc_batched(gre_graph g, const std::vector<uint32_t>& hs, double* dbc,
   const ChunkTable& T = g->bc_chunks;
   double *sigma, *dep, *partial;
   uint32_t *list, *srcs;
-  unsigned long long *seen, *cnt;
+  unsigned long long *seen, *cnt, *acc;
   GRE_CHECK(ws_array(g, WS_BC1, n * 64, &sigma));
   GRE_CHECK(ws_array(g, WS_BC2, n * 64, &dep));
   GRE_CHECK(ws_array(g, WS_BC3, n, &list));
   GRE_CHECK(ws_array(g, WS_BC4, n, &seen));
   GRE_CHECK(ws_array(g, WS_BC5, (T.nchunks + 1) * 64, &partial));
-  GRE_CHECK(ws_array(g, WS_BC6, 4, &cnt));
+  GRE_CHECK(ws_array(g, WS_BC6, 8, &cnt));
+  GRE_CHECK(ensure_bins(g, true));
+  GRE_CHECK(ws_array(g, WS_BC0, n, &acc));
+  GRE_CUDA(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * n, g->stream));
   GRE_CHECK(ws_array(g, WS_BC7, 64, &srcs));
   GRE_CHECK(fpool_levels(g, 32));
   uint64_t arcs = 0, bytes = 0;
@@ -440,14 +470,29 @@ static int bc_batched(gre_graph g, const std::vector<uint32_t>& hs, double* dbc,
       GRE_CHECK(fpool_levels(g, nl + 1));
       unsigned long long* fd = (unsigned long long*)g->bc_fpool + (nl - 1) * n;
       unsigned long long* fn = (unsigned long long*)g->bc_fpool + nl * n;
-      GRE_CUDA(cudaMemsetAsync(cnt, 0, 16, g->stream));
-      k_bcm_forward<<<grid_for(n, 256, 8), 256, 0, g->stream>>>(n, full, g->roff, g->rcol, fd, fn, seen, cnt);
+      // push from a sparse frontier, pull otherwise (same frontier words either way)
+      GRE_CUDA(cudaMemsetAsync(cnt, 0, 64, g->stream));
+      ms::k_frontier_list<<<grid_for(n, 256, 8), 256, 0, g->stream>>>(n, fd, g->off, list, (unsigned int*)(cnt + 2), cnt + 3);
+      unsigned long long h[5];
+      GRE_CUDA(cudaMemcpyAsync(h, cnt, sizeof(unsigned long long) * 4, cudaMemcpyDeviceToHost, g->stream));
+      GRE_CUDA(cudaStreamSynchronize(g->stream));
+      const bool push = h[3] * 14 < g->m;
+      if (push)
+        ms::k_push<<<grid_for((h[2] & 0xffffffffull) * 32, 256, 8), 256, 0, g->stream>>>(list, (unsigned int*)(cnt + 2), g->off,
+                                                                                          g->col, fd, seen, acc);
+      else
+        GRE_CHECK(ms::pull(g->bins_in, full, g->roff, g->rcol, fd, seen, acc, cnt + 4, g->stream));
+      ms::k_commit<<<grid_for(n, 256, 8), 256, 0, g->stream>>>(n, acc, seen, fn, nullptr, 0, cnt);
       GRE_LAUNCH_CHECK();
-      unsigned long long h[2];
       GRE_CUDA(cudaMemcpyAsync(h, cnt, sizeof h, cudaMemcpyDeviceToHost, g->stream));
       GRE_CUDA(cudaStreamSynchronize(g->stream));
-      arcs += h[1];
-      bytes += 24 * n + 12 * h[1];
+      if (push) {
+        arcs += h[3];
+        bytes += 16 * (h[2] & 0xffffffffull) + 12 * h[3] + 32 * n;
+      } else {
+        arcs += h[4];
+        bytes += 24 * n + 12 * h[4];
+      }
       if (h[0] == 0) break;
       ++nl;
     }

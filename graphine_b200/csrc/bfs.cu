@@ -25,6 +25,7 @@
 #include <algorithm>
 
 #include "gre_internal.cuh"
+#include "msbfs.cuh"
 
 namespace gre {
 
@@ -448,10 +449,16 @@ int gre_msbfs(gre_graph g, const uint32_t* srcs, uint32_t nsrc, int32_t* levels,
   GRE_CHECK(ws_array(g, WS_A, n, &seen));
   GRE_CHECK(ws_array(g, WS_B, n, &fa));
   GRE_CHECK(ws_array(g, WS_C, n, &fb));
+  unsigned long long* acc;
+  uint32_t* flist;
   GRE_CHECK(ws_array(g, WS_D, 64, &dsrc));
-  GRE_CHECK(ws_array(g, WS_COUNTERS, 4, &cnt));
+  GRE_CHECK(ws_array(g, WS_E, n, &acc));
+  GRE_CHECK(ws_array(g, WS_F, n, &flist));
+  GRE_CHECK(ws_array(g, WS_COUNTERS, 8, &cnt));
+  GRE_CHECK(ensure_bins(g, true));
   RunTimer timer(g);
   GRE_CUDA(cudaMemsetAsync(dl, 0xff, sizeof(int32_t) * nsrc * n, g->stream));
+  GRE_CUDA(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * n, g->stream));
   uint64_t scanned = 0, bytes = 0;
   uint32_t max_levels = 0;
   for (uint32_t j0 = 0; j0 < nsrc; j0 += 64) {
@@ -465,17 +472,33 @@ int gre_msbfs(gre_graph g, const uint32_t* srcs, uint32_t nsrc, int32_t* levels,
     unsigned long long* front = fa;
     unsigned long long* next = fb;
     for (int32_t d = 0;; ++d) {
-      GRE_CUDA(cudaMemsetAsync(cnt, 0, 16, g->stream));
-      k_ms_pull<<<grid_for(n, 256, 8), 256, 0, g->stream>>>(n, k, full, g->roff, g->rcol, front, next, seen, lv, d + 1, cnt);
+      // direction: push when the frontier's arcs are few (Beamer's rule against all arcs)
+      GRE_CUDA(cudaMemsetAsync(cnt, 0, 64, g->stream));
+      ms::k_frontier_list<<<grid_for(n, 256, 8), 256, 0, g->stream>>>(n, front, g->off, flist, (unsigned int*)(cnt + 2), cnt + 3);
+      unsigned long long h[5];
+      GRE_CUDA(cudaMemcpyAsync(h, cnt, sizeof(unsigned long long) * 4, cudaMemcpyDeviceToHost, g->stream));
+      GRE_CUDA(cudaStreamSynchronize(g->stream));
+      const bool push = h[3] * 14 < g->m;
+      if (push)
+        ms::k_push<<<grid_for((h[2] & 0xffffffffull) * 32, 256, 8), 256, 0, g->stream>>>(flist, (unsigned int*)(cnt + 2), g->off,
+                                                                                          g->col, front, seen, acc);
+      else
+        GRE_CHECK(ms::pull(g->bins_in, full, g->roff, g->rcol, front, seen, acc, cnt + 4, g->stream));
+      ms::k_commit<<<grid_for(n, 256, 8), 256, 0, g->stream>>>(n, acc, seen, next, lv, d + 1, cnt);
       GRE_LAUNCH_CHECK();
-      unsigned long long h[2];
       GRE_CUDA(cudaMemcpyAsync(h, cnt, sizeof h, cudaMemcpyDeviceToHost, g->stream));
       GRE_CUDA(cudaStreamSynchronize(g->stream));
-      scanned += h[1];
-      bytes += 24 * n + 12 * h[1];
+      const unsigned long long found_bits = h[1];
+      if (push) {
+        scanned += h[3];
+        bytes += 16 * (h[2] & 0xffffffffull) + 12 * h[3] + 32 * n;
+      } else {
+        scanned += h[4];
+        bytes += 24 * n + 12 * h[4];
+      }
       std::swap(front, next);
-      if (nsrc <= 64) stats_record(st, h[0]);
-      if (h[0] == 0) {
+      if (nsrc <= 64) stats_record(st, found_bits);
+      if (found_bits == 0) {
         max_levels = std::max<uint32_t>(max_levels, (uint32_t)d);
         break;
       }

@@ -160,7 +160,9 @@ __global__ void __launch_bounds__(256) k_ppr_rows(const uint32_t* __restrict__ r
   for (uint64_t i = warp; i < count; i += nwarps) {
     const uint32_t v = rows[i];
     double acc[kCols / 32] = {0.0, 0.0, 0.0, 0.0};
-    R.accumulate(R.roff[v], R.roff[v + 1], acc);
+    const uint64_t a0 = R.roff[v], a1 = R.roff[v + 1];
+    if (a1 - a0 > kPprChunk) continue;  // chunked (uniform: one row per warp)
+    R.accumulate(a0, a1, acc);
     F(v, acc);
   }
 }
@@ -217,32 +219,42 @@ struct PprChunks {
 };
 
 static int ppr_chunks(gre_graph g, PprChunks* pc) {
+  // candidates: rows of more than 64 arcs (bins 5..7, contiguous in the bin list); only those
+  // longer than kPprChunk are chunked, the others stay with the warp-per-row kernel
   const DegreeBins& B = g->bins_in;
-  pc->nrows = B.count[5] + B.count[6] + B.count[7];  // rows longer than 64 arcs
-  pc->rows = B.rows + B.start[5];
-  if (!pc->nrows) return GRE_SUCCESS;
-  std::vector<uint32_t> rows(pc->nrows);
+  const uint64_t cand = B.count[5] + B.count[6] + B.count[7];
+  pc->nrows = 0;
+  pc->nchunks = 0;
+  if (!cand) return GRE_SUCCESS;
+  std::vector<uint32_t> rows(cand), lrows;
   std::vector<uint64_t> ho(g->n + 1);
-  GRE_CUDA(cudaMemcpy(rows.data(), pc->rows, sizeof(uint32_t) * pc->nrows, cudaMemcpyDeviceToHost));
+  GRE_CUDA(cudaMemcpy(rows.data(), B.rows + B.start[5], sizeof(uint32_t) * cand, cudaMemcpyDeviceToHost));
   GRE_CUDA(cudaMemcpy(ho.data(), g->roff, sizeof(uint64_t) * (g->n + 1), cudaMemcpyDeviceToHost));
   std::vector<uint64_t> crow, cbeg, first;
-  for (uint64_t i = 0; i < pc->nrows; ++i) {
+  for (uint64_t i = 0; i < cand; ++i) {
+    const uint32_t v = rows[i];
+    if (ho[v + 1] - ho[v] <= kPprChunk) continue;
     first.push_back(crow.size());
-    for (uint64_t a = ho[rows[i]]; a < ho[rows[i] + 1]; a += kPprChunk) {
-      crow.push_back(i);
+    for (uint64_t a = ho[v]; a < ho[v + 1]; a += kPprChunk) {
+      crow.push_back(lrows.size());
       cbeg.push_back(a);
     }
+    lrows.push_back(v);
   }
   first.push_back(crow.size());
+  pc->nrows = lrows.size();
   pc->nchunks = crow.size();
+  if (!pc->nrows) return GRE_SUCCESS;
   void* p;
-  GRE_CHECK(g->ws.get(WS_L, sizeof(uint64_t) * (crow.size() * 2 + first.size()), &p));
+  GRE_CHECK(g->ws.get(WS_L, sizeof(uint64_t) * (crow.size() * 2 + first.size()) + sizeof(uint32_t) * lrows.size(), &p));
   pc->row = (uint64_t*)p;
   pc->begin = pc->row + crow.size();
   pc->first = pc->begin + crow.size();
+  pc->rows = (uint32_t*)(pc->first + first.size());
   GRE_CUDA(cudaMemcpyAsync(pc->row, crow.data(), sizeof(uint64_t) * crow.size(), cudaMemcpyHostToDevice, g->stream));
   GRE_CUDA(cudaMemcpyAsync(pc->begin, cbeg.data(), sizeof(uint64_t) * cbeg.size(), cudaMemcpyHostToDevice, g->stream));
   GRE_CUDA(cudaMemcpyAsync(pc->first, first.data(), sizeof(uint64_t) * first.size(), cudaMemcpyHostToDevice, g->stream));
+  GRE_CUDA(cudaMemcpyAsync(pc->rows, lrows.data(), sizeof(uint32_t) * lrows.size(), cudaMemcpyHostToDevice, g->stream));
   GRE_CUDA(cudaStreamSynchronize(g->stream));
   return GRE_SUCCESS;
 }
@@ -512,7 +524,7 @@ int gre_ppr(gre_graph g, const uint32_t* seeds, uint32_t k, double d, uint32_t i
     GRE_CHECK(ws_array(g, WS_E, kCols, &dseeds));
     const DegreeBins& B = g->bins_in;
     uint64_t short_rows = 0;
-    for (int b = 0; b < 5; ++b) short_rows += B.count[b];
+    for (int b = 0; b < 6; ++b) short_rows += B.count[b];  // rows longer than kPprChunk are skipped
     for (uint32_t j0 = 0; j0 < k; j0 += kCols) {
       const uint32_t kk = (k - j0) < (uint32_t)kCols ? (k - j0) : (uint32_t)kCols;
       GRE_CUDA(cudaMemcpyAsync(dseeds, hs.data() + j0, sizeof(uint32_t) * kk, cudaMemcpyHostToDevice, g->stream));
