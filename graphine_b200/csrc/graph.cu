@@ -932,6 +932,7 @@ int gre_graph_set_weights_u32(gre_graph g, const uint32_t* w) {
   GRE_CHECK(use_graph(g));
   if (!g->w32) GRE_CUDA(cudaMalloc(&g->w32, sizeof(uint32_t) * (g->m ? g->m : 1)));
   GRE_CHECK(upload_arcs(g, w, 4, g->w32));
+  g->w32_mean = -1.0;
   GRE_CUDA(cudaStreamSynchronize(g->stream));
   return GRE_SUCCESS;
 }
@@ -942,6 +943,7 @@ int gre_graph_set_weights_hash(gre_graph g, uint64_t wseed) {
   if (!g->w32) GRE_CUDA(cudaMalloc(&g->w32, sizeof(uint32_t) * (g->m ? g->m : 1)));
   if (g->m) k_hash_weights<<<grid_for(g->m, 256), 256, 0, g->stream>>>(g->n, g->m, g->off, g->col, g->perm, wseed, g->w32);
   GRE_LAUNCH_CHECK();
+  g->w32_mean = -1.0;
   GRE_CUDA(cudaStreamSynchronize(g->stream));
   return GRE_SUCCESS;
 }

@@ -104,6 +104,7 @@ struct gre_graph_s {
   uint32_t* indeg = nullptr;  // aliases outdeg when symmetric
   // weights
   uint32_t* w32 = nullptr;
+  double w32_mean = -1.0;  // mean of w32, computed on first use (-1: unknown)
   double* w64 = nullptr;
   double* rw64 = nullptr;  // FP64 weights in CSC order (built on demand)
   uint64_t max_outdeg = 0, max_indeg = 0;

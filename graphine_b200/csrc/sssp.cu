@@ -1,22 +1,29 @@
-// SSSP fast path: frontier relaxation with uint32 weights.
+// SSSP fast path: near-far frontier relaxation with uint32 weights.
 //
 // Same fixed point as the reference SSSP plugin (Kernels/SSSP.hpp:55-89: scatter last[u]+w,
 // combine = min, every improved vertex re-activated): shortest-path distances are unique, so
 // the result is bit-exact whatever the relaxation order.  Differences from the reference's
 // superstep, chosen for the GPU:
-//   * the frontier is a queue of improved vertices, expanded edge-balanced (one thread per
-//     frontier arc, owner found by binary search in the scan of frontier degrees), so hubs do
-//     not serialise a warp;
-//   * the distance of the frontier vertex is read when its arc is relaxed (not a copy taken
-//     at the start of the superstep), which can only lower the values sent and converges in
-//     at most as many supersteps;
-//   * a bitmap de-duplicates the next frontier (one queue slot per improved vertex).
+//   * near-far ordering (Davidson et al., IPDPS 2014): improved vertices below a moving limit
+//     form the next frontier, the others wait in a far pile until the limit (raised by a bucket
+//     width delta, or to the smallest waiting distance + delta) passes them.  This cuts the
+//     re-relaxations of a plain Bellman-Ford frontier (delta = 0) roughly in half on RMAT;
+//   * the frontier is expanded edge-balanced in tiles of 2048 consecutive frontier arcs (the
+//     owners staged in shared memory, owner of each arc by a block max-scan), so hubs do not
+//     serialise a warp;
+//   * an improvement is a fire-and-forget atomic min on the distance plus a bit in a changed
+//     bitmap: no thread waits for an atomic's reply (hub heads receive thousands per superstep),
+//     and a pass over the bitmap builds the next frontier and far pile without duplicates;
+//   * the distance of a frontier vertex is read when its tile starts (not a copy taken at the
+//     start of the superstep), which can only lower the values sent;
+//   * vertices without out-arcs are never queued (they have nothing to relax).
 //
 // Byte model per superstep: 16 F (queue + offsets) + 12 A (column + weight + dist probe)
 // + 8 N (queue append + bitmap), F frontier, A arcs relaxed, N improved vertices.
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "gre_internal.cuh"
 
@@ -37,102 +44,336 @@ __global__ void k_sssp_seed(uint32_t src, uint32_t* __restrict__ dist, uint32_t*
   }
 }
 
-__global__ void k_sssp_degrees(const uint32_t* __restrict__ queue, uint64_t nq, const uint64_t* __restrict__ off,
+// Degrees of the queued vertices, for the scan.
+__global__ void k_sssp_degrees(const uint32_t* __restrict__ queue, uint64_t nq, const uint32_t* __restrict__ outdeg,
                                uint64_t* __restrict__ deg) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nq; i += (uint64_t)gridDim.x * blockDim.x)
+    deg[i] = outdeg[queue[i]];
+}
+
+// Edge-balanced expansion in tiles of kTile consecutive frontier arcs.  k_tile_starts records,
+// for every tile, the frontier index owning its first arc (each frontier vertex writes the
+// tiles that begin inside its arc range, so every entry is written exactly once).  A CTA then
+// stages the owners of its tile (at most kTile + 1 of them, since queued vertices have at least
+// one out-arc) in shared memory and each thread finds the owner of its arc there: the per-arc
+// search touches shared memory only, and the column and weight reads of one vertex coalesce.
+// Queue appends are gathered per tile in shared memory and reserved with one global atomic per
+// tile, so the queue counters are not a point of contention.
+constexpr int kTileThreads = 256;
+constexpr int kTileItems = 8;
+constexpr uint64_t kTile = (uint64_t)kTileThreads * kTileItems;
+static_assert(kTileItems == 8, "owner scan packs 8 uint16 per thread");
+
+struct MaxOp {
+  __device__ __forceinline__ uint32_t operator()(uint32_t a, uint32_t b) const { return a > b ? a : b; }
+};
+
+__global__ void k_tile_starts(const uint64_t* __restrict__ prefix, uint64_t nq, uint32_t* __restrict__ start) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nq; i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t u = queue[i];
-    deg[i] = off[u + 1] - off[u];
+    const uint64_t p0 = prefix[i], p1 = prefix[i + 1];
+    if (p1 == p0) continue;
+    for (uint64_t t = (p0 + kTile - 1) / kTile; t <= (p1 - 1) / kTile; ++t) start[t] = (uint32_t)i;
   }
 }
 
-__global__ void __launch_bounds__(256) k_sssp_relax(const uint32_t* __restrict__ queue, uint64_t nq, const uint64_t* __restrict__ prefix,
-                                                    uint64_t total, const uint64_t* __restrict__ off, const uint32_t* __restrict__ col,
-                                                    const uint32_t* __restrict__ w, uint32_t* __restrict__ dist,
-                                                    uint32_t* __restrict__ inq, uint32_t* __restrict__ next_queue,
-                                                    uint32_t* __restrict__ next_count) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t base = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) & ~31ull; base < total; base += stride) {
-    const uint64_t t = base + (threadIdx.x & 31u);
-    bool push = false;
-    uint32_t v = 0;
-    if (t < total) {
-      uint64_t lo = 0, hi = nq;
-      while (hi - lo > 1) {
-        const uint64_t mid = (lo + hi) >> 1;
-        if (prefix[mid] <= t) lo = mid;
-        else hi = mid;
+__global__ void __launch_bounds__(kTileThreads) k_sssp_relax(const uint32_t* __restrict__ queue, uint64_t nq,
+                                                             const uint64_t* __restrict__ prefix, uint64_t total, const uint32_t* __restrict__ start,
+                                                             const uint64_t* __restrict__ off, const uint32_t* __restrict__ col,
+                                                             const uint32_t* __restrict__ w, uint32_t* __restrict__ dist,
+                                                             uint32_t* __restrict__ changed, uint32_t* __restrict__ error) {
+  using OwnerScan = cub::BlockScan<uint32_t, kTileThreads>;
+  __shared__ uint64_t s_arc[kTile + 1];                // arc index at tile position s_rel[j]
+  __shared__ uint32_t s_du[kTile + 1];                 // distance of owner j
+  __shared__ uint16_t s_rel[kTile + 1];                // first tile position of owner j
+  __shared__ __align__(16) uint16_t s_own[kTile];      // owner of each tile position
+  __shared__ typename OwnerScan::TempStorage s_scan;
+  const uint64_t ntiles = (total + kTile - 1) / kTile;
+  for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const uint64_t t0 = tile * kTile;
+    const uint32_t len = (uint32_t)(total - t0 < kTile ? total - t0 : kTile);
+    const uint64_t lo = start[tile];
+    const uint64_t hi = tile + 1 < ntiles ? start[tile + 1] : nq - 1;
+    const uint64_t cnt = hi - lo + 1;
+    if (cnt > kTile + 1) {  // cannot happen while every queued vertex has an out-arc; uniform
+      if (threadIdx.x == 0) atomicOr(error, 1u);
+      continue;
+    }
+    *(uint4*)(s_own + threadIdx.x * kTileItems) = make_uint4(0, 0, 0, 0);
+    for (uint64_t j = threadIdx.x; j < cnt; j += kTileThreads) {
+      const uint32_t u = queue[lo + j];
+      const uint64_t p = prefix[lo + j];
+      const uint64_t r = p > t0 ? p - t0 : 0;
+      s_rel[j] = (uint16_t)r;
+      s_arc[j] = off[u] + (t0 + r - p);
+      s_du[j] = __ldcg(dist + u);
+    }
+    __syncthreads();
+    // owner of every tile position: mark where each owner's arcs begin, then a running maximum
+    // (owners begin at strictly increasing positions, every queued vertex having an out-arc)
+    for (uint32_t j = 1 + threadIdx.x; j < cnt; j += kTileThreads)
+      if (s_rel[j] < len) s_own[s_rel[j]] = (uint16_t)j;
+    __syncthreads();
+    {
+      uint32_t own[kTileItems];
+      const uint4 raw = *(const uint4*)(s_own + threadIdx.x * kTileItems);
+      const uint32_t wds[4] = {raw.x, raw.y, raw.z, raw.w};
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        own[2 * k] = wds[k] & 0xffffu;
+        own[2 * k + 1] = wds[k] >> 16;
       }
-      const uint32_t u = queue[lo];
-      const uint64_t a = off[u] + (t - prefix[lo]);
-      v = __ldg(col + a);
-      const uint32_t nd = *(volatile uint32_t*)(dist + u) + __ldg(w + a);
-      if (nd < *(volatile uint32_t*)(dist + v)) {
-        const uint32_t old = atomicMin(dist + v, nd);
-        if (nd < old) {
-          const uint32_t bit = 1u << (v & 31u);
-          const uint32_t prev = atomicOr(inq + (v >> 5), bit);
-          push = !(prev & bit);
-        }
+      OwnerScan(s_scan).InclusiveScan(own, own, MaxOp());
+      *(uint4*)(s_own + threadIdx.x * kTileItems) =
+          make_uint4(own[0] | own[1] << 16, own[2] | own[3] << 16, own[4] | own[5] << 16, own[6] | own[7] << 16);
+    }
+    __syncthreads();
+    // the thread's kTileItems arcs in rounds of independent loads (column and weight, then the
+    // head's distance); an improvement is a fire-and-forget atomic min plus a bit in `changed`,
+    // so no thread waits for an atomic's reply (hub heads receive many of them)
+    uint32_t du[kTileItems], v[kTileItems], wt[kTileItems], dv[kTileItems];
+#pragma unroll
+    for (int k = 0; k < kTileItems; ++k) {
+      const uint32_t t = (uint32_t)k * kTileThreads + threadIdx.x;
+      const uint32_t a = s_own[t];
+      const uint64_t arc = s_arc[a] + (t - s_rel[a]);
+      du[k] = s_du[a];
+      const bool ok = t < len;
+      v[k] = ok ? __ldg(col + arc) : 0u;
+      wt[k] = ok ? __ldg(w + arc) : 0u;
+    }
+#pragma unroll
+    for (int k = 0; k < kTileItems; ++k) {
+      const bool ok = (uint32_t)k * kTileThreads + threadIdx.x < len;
+      dv[k] = ok ? __ldcg(dist + v[k]) : 0u;
+    }
+#pragma unroll
+    for (int k = 0; k < kTileItems; ++k) {
+      const bool ok = (uint32_t)k * kTileThreads + threadIdx.x < len;
+      const uint32_t nd = du[k] + wt[k];
+      if (ok && nd < dv[k]) {
+        atomicMin(dist + v[k], nd);
+        atomicOr(changed + (v[k] >> 5), 1u << (v[k] & 31u));
       }
     }
-    const uint32_t pos = warp_append(next_count, push);
-    if (push) next_queue[pos] = v;
+    __syncthreads();
   }
 }
 
-__global__ void k_sssp_clear_bits(const uint32_t* __restrict__ queue, uint64_t nq, uint32_t* __restrict__ inq) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nq; i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t v = queue[i];
-    atomicAnd(inq + (v >> 5), ~(1u << (v & 31u)));
+// Changed vertices -> next queues, one lane per bitmap word (the word is cleared).  A vertex
+// without out-arcs is dropped (nothing to relax).  Below the limit it joins the near queue (and
+// its far entry, if any, becomes void); otherwise it joins the far pile unless already there.
+__global__ void k_sssp_classify(uint64_t nwords, uint32_t* __restrict__ changed, const uint32_t* __restrict__ dist,
+                                const uint32_t* __restrict__ outdeg, uint32_t near_limit, uint32_t* __restrict__ near,
+                                uint32_t* __restrict__ infar, uint32_t* __restrict__ far, uint32_t* __restrict__ counters) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) & ~31ull; base < nwords; base += stride) {
+    const uint64_t wi = base + (threadIdx.x & 31u);
+    uint32_t bits = 0, fbits = 0;
+    if (wi < nwords) {
+      bits = changed[wi];
+      if (bits) {
+        changed[wi] = 0;
+        fbits = infar[wi];
+      }
+    }
+    uint32_t set_far = 0, clear_far = 0;
+    while (__any_sync(0xffffffffu, bits != 0)) {
+      bool to_near = false, to_far = false;
+      uint32_t v = 0;
+      if (bits) {
+        const uint32_t b = __ffs(bits) - 1;
+        bits &= bits - 1;
+        v = (uint32_t)(wi << 5) + b;
+        if (__ldg(outdeg + v) != 0) {
+          if (dist[v] < near_limit) {
+            to_near = true;
+            if (fbits & (1u << b)) clear_far |= 1u << b;
+          } else if (!(fbits & (1u << b))) {
+            to_far = true;
+            set_far |= 1u << b;
+          }
+        }
+      }
+      const uint32_t p = warp_append(counters, to_near);
+      if (to_near) near[p] = v;
+      const uint32_t f = warp_append(counters + 2, to_far);
+      if (to_far) far[f] = v;
+    }
+    if (set_far | clear_far) infar[wi] = (fbits | set_far) & ~clear_far;  // one lane owns the word
   }
 }
 
-static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bool record) {
+// Near-far pile split: far vertices whose distance is now below the limit move to the near
+// queue (their far bit is cleared), the others stay; entries whose far bit was cleared (the
+// vertex went to the near queue since) are dropped.  counters[3] gets the smallest distance left.
+__global__ void k_far_split(const uint32_t* __restrict__ far, uint64_t nfar, const uint32_t* __restrict__ dist, uint32_t near_limit,
+                            uint32_t* __restrict__ infar, uint32_t* __restrict__ near, uint32_t* __restrict__ far_out,
+                            uint32_t* __restrict__ counters) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  uint32_t dmin = 0xffffffffu;
+  for (uint64_t base = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) & ~31ull; base < nfar; base += stride) {
+    const uint64_t i = base + (threadIdx.x & 31u);
+    bool to_near = false, keep = false;
+    uint32_t v = 0;
+    if (i < nfar) {
+      v = far[i];
+      const uint32_t bit = 1u << (v & 31u);
+      if (infar[v >> 5] & bit) {
+        const uint32_t d = dist[v];
+        to_near = d < near_limit;
+        keep = !to_near;
+        if (to_near) atomicAnd(infar + (v >> 5), ~bit);
+        else dmin = min(dmin, d);
+      }
+    }
+    const uint32_t p = warp_append(counters, to_near);
+    if (to_near) near[p] = v;
+    const uint32_t k = warp_append(counters + 2, keep);
+    if (keep) far_out[k] = v;
+  }
+  dmin = __reduce_min_sync(0xffffffffu, dmin);
+  if ((threadIdx.x & 31u) == 0 && dmin != 0xffffffffu) atomicMin(counters + 3, dmin);
+}
+
+struct AddU64 {
+  __device__ __forceinline__ uint64_t operator()(uint64_t a, uint64_t b) const { return a + b; }
+};
+
+// Bucket width of the near-far split.  Default: half the mean arc weight (unit weights give
+// one bucket per BFS level); 0 relaxes every improved vertex at once (Bellman-Ford frontier).
+// The GRE_SSSP_DELTA environment variable overrides it.
+static int sssp_delta(gre_graph g, uint32_t* delta) {
+  if (const char* e = getenv("GRE_SSSP_DELTA")) {
+    *delta = (uint32_t)strtoul(e, nullptr, 10);
+    return GRE_SUCCESS;
+  }
+  if (g->w32_mean < 0) {
+    uint64_t* dsum = nullptr;
+    GRE_CHECK(ws_array(g, WS_COUNTERS, 1, &dsum));
+    size_t tb = 0;
+    cub::DeviceReduce::Reduce(nullptr, tb, g->w32, dsum, g->m, AddU64(), (uint64_t)0, g->stream);
+    void* tmp = nullptr;
+    GRE_CHECK(g->ws.get(WS_CUB, tb, &tmp));
+    GRE_CUDA(cub::DeviceReduce::Reduce(tmp, tb, g->w32, dsum, g->m, AddU64(), (uint64_t)0, g->stream));
+    uint64_t sum = 0;
+    GRE_CUDA(cudaMemcpyAsync(&sum, dsum, sizeof sum, cudaMemcpyDeviceToHost, g->stream));
+    GRE_CUDA(cudaStreamSynchronize(g->stream));
+    g->w32_mean = g->m ? (double)sum / (double)g->m : 1.0;
+  }
+  const double d = g->w32_mean / 2.0;
+  *delta = d < 1.0 ? 1u : d > 1e9 ? 1000000000u : (uint32_t)d;
+  return GRE_SUCCESS;
+}
+
+// counters: [0] near appends, [1] overflow flag, [2] far appends (starts at the current far
+// pile size, which the classification extends), [3] unused here
+static int init_counters(gre_graph g, uint32_t* cnt, const uint32_t* init, uint32_t nfar) {
+  const uint32_t h[4] = {init[0], init[1], nfar, init[3]};  // pageable: staged before the call returns
+  GRE_CUDA(cudaMemcpyAsync(cnt, h, sizeof h, cudaMemcpyHostToDevice, g->stream));
+  return GRE_SUCCESS;
+}
+
+// Resident CTAs of the relaxation kernel per SM: the grid is exactly one wave, so that no
+// CTA starts its tiles late.
+static int relax_blocks_per_sm() {
+  static int per_sm = 0;
+  if (!per_sm) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sssp_relax, kTileThreads, 0) != cudaSuccess || b < 1) b = 1;
+    per_sm = b;
+  }
+  return per_sm;
+}
+
+static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bool record, uint32_t delta) {
   const uint64_t n = g->n;
   const uint64_t nwords = (n + 31) >> 5;
-  uint32_t *qa, *qb, *inq, *cnt;
+  uint32_t *qa, *qb, *changed, *cnt, *fa, *fb, *infar, *tstart;
   uint64_t *deg, *prefix;
   GRE_CHECK(ws_array(g, WS_A, n, &qa));
   GRE_CHECK(ws_array(g, WS_B, n, &qb));
-  GRE_CHECK(ws_array(g, WS_C, nwords, &inq));
+  GRE_CHECK(ws_array(g, WS_C, nwords, &changed));
+  GRE_CHECK(ws_array(g, WS_D, n, &fa));
+  GRE_CHECK(ws_array(g, WS_E, n, &fb));
   GRE_CHECK(ws_array(g, WS_F, n + 1, &deg));
   GRE_CHECK(ws_array(g, WS_G, n + 1, &prefix));
+  GRE_CHECK(ws_array(g, WS_I, g->m / kTile + 2, &tstart));
+  GRE_CHECK(ws_array(g, WS_J, nwords, &infar));
   GRE_CHECK(ws_array(g, WS_COUNTERS, 4, &cnt));
   size_t cubbytes = 0;
   void* cubtmp = nullptr;
   cub::DeviceScan::ExclusiveSum(nullptr, cubbytes, deg, prefix, n + 1, g->stream);
   GRE_CHECK(g->ws.get(WS_CUB, cubbytes, &cubtmp));
   GRE_CUDA(cudaMemsetAsync(dist, 0xff, sizeof(uint32_t) * n, g->stream));
-  GRE_CUDA(cudaMemsetAsync(inq, 0, sizeof(uint32_t) * nwords, g->stream));
+  GRE_CUDA(cudaMemsetAsync(changed, 0, sizeof(uint32_t) * nwords, g->stream));
+  GRE_CUDA(cudaMemsetAsync(infar, 0, sizeof(uint32_t) * nwords, g->stream));
   k_sssp_seed<<<1, 32, 0, g->stream>>>(src, dist, qa);
-  uint64_t nq = 1, relaxed = 0, bytes = 0;
+  uint32_t limit = delta ? delta : 0xffffffffu;
+  uint64_t nq = 1, nfar = 0, relaxed = 0, bytes = 0;
   uint32_t* q = qa;
   uint32_t* nqueue = qb;
+  uint32_t* far = fa;
+  uint32_t* far2 = fb;
   uint32_t steps = 0;
   const int sms = num_sms();
-  while (nq > 0) {
-    k_sssp_degrees<<<grid_for(nq, 256), 256, 0, g->stream>>>(q, nq, g->off, deg);
-    GRE_CUDA(cub::DeviceScan::ExclusiveSum(cubtmp, cubbytes, deg, prefix, nq + 1, g->stream));
-    GRE_CUDA(cudaMemsetAsync(cnt, 0, 4, g->stream));
-    uint64_t total = 0;
-    GRE_CUDA(cudaMemcpyAsync(&total, prefix + nq, sizeof total, cudaMemcpyDeviceToHost, g->stream));
-    GRE_CUDA(cudaStreamSynchronize(g->stream));
-    // vertices leave the queue: they may be re-queued by this superstep's relaxations
-    k_sssp_clear_bits<<<grid_for(nq, 256), 256, 0, g->stream>>>(q, nq, inq);
-    if (total) {
-      const int grid = (int)std::min<uint64_t>((total + 255) / 256, (uint64_t)sms * 16);
-      k_sssp_relax<<<grid, 256, 0, g->stream>>>(q, nq, prefix, total, g->off, g->col, g->w32, dist, inq, nqueue, cnt);
+  const uint32_t init[4] = {0, 0, 0, 0xffffffffu};
+  for (;;) {
+    while (nq > 0) {
+      k_sssp_degrees<<<grid_for(nq, 256), 256, 0, g->stream>>>(q, nq, g->outdeg, deg);
+      GRE_CUDA(cub::DeviceScan::ExclusiveSum(cubtmp, cubbytes, deg, prefix, nq + 1, g->stream));
+      uint64_t total = 0;
+      GRE_CUDA(cudaMemcpyAsync(&total, prefix + nq, sizeof total, cudaMemcpyDeviceToHost, g->stream));
+      GRE_CUDA(cudaStreamSynchronize(g->stream));
+      GRE_CHECK(init_counters(g, cnt, init, (uint32_t)nfar));
+      if (total) {
+        const uint64_t ntiles = (total + kTile - 1) / kTile;
+        k_tile_starts<<<grid_for(nq, 256), 256, 0, g->stream>>>(prefix, nq, tstart);
+        // the arc count is a launch argument: read inside the kernel instead, the relaxation
+        // measured 1.7x slower on RMAT-26
+        const int grid = (int)std::min<uint64_t>(ntiles, (uint64_t)sms * relax_blocks_per_sm());
+        k_sssp_relax<<<grid, kTileThreads, 0, g->stream>>>(q, nq, prefix, total, tstart, g->off, g->col, g->w32, dist, changed,
+                                                            cnt + 1);
+        k_sssp_classify<<<grid_for(nwords, 256, 8), 256, 0, g->stream>>>(nwords, changed, dist, g->outdeg, limit, nqueue, infar,
+                                                                          far, cnt);
+      }
+      GRE_LAUNCH_CHECK();
+      uint32_t h[4];
+      GRE_CUDA(cudaMemcpyAsync(h, cnt, sizeof h, cudaMemcpyDeviceToHost, g->stream));
+      GRE_CUDA(cudaStreamSynchronize(g->stream));
+      if (h[1]) {
+        set_error("gre_sssp: frontier tile overflow");
+        return GRE_FAILURE;
+      }
+      relaxed += total;
+      bytes += 16 * nq + 12 * total + 8 * (uint64_t)(h[0] + h[2] - nfar);
+      nq = h[0];
+      nfar = h[2];
+      std::swap(q, nqueue);
+      ++steps;
+      if (record) stats_record(st, nq);
     }
-    GRE_LAUNCH_CHECK();
-    uint32_t h = 0;
-    GRE_CUDA(cudaMemcpyAsync(&h, cnt, 4, cudaMemcpyDeviceToHost, g->stream));
-    GRE_CUDA(cudaStreamSynchronize(g->stream));
-    relaxed += total;
-    bytes += 16 * nq + 12 * total + 8 * (uint64_t)h;
-    nq = h;
-    std::swap(q, nqueue);
-    ++steps;
-    if (record) stats_record(st, nq);
+    if (nfar == 0) break;
+    // the near queue is empty: raise the limit (past empty buckets) and pull the far vertices below it
+    uint32_t lowest = 0;
+    for (int pass = 0; nq == 0 && nfar > 0; ++pass) {
+      if (pass == 2) {  // the second pass starts at the smallest distance left: cannot come back empty
+        set_error("gre_sssp: near-far split made no progress");
+        return GRE_FAILURE;
+      }
+      if (pass == 0) limit = limit > 0xffffffffu - delta ? 0xffffffffu : limit + delta;
+      else limit = lowest > 0xffffffffu - delta ? 0xffffffffu : lowest + delta;
+      GRE_CUDA(cudaMemcpyAsync(cnt, init, sizeof init, cudaMemcpyHostToDevice, g->stream));
+      k_far_split<<<grid_for(nfar, 256, 8), 256, 0, g->stream>>>(far, nfar, dist, limit, infar, q, far2, cnt);
+      GRE_LAUNCH_CHECK();
+      uint32_t h[4];
+      GRE_CUDA(cudaMemcpyAsync(h, cnt, sizeof h, cudaMemcpyDeviceToHost, g->stream));
+      GRE_CUDA(cudaStreamSynchronize(g->stream));
+      bytes += 8 * nfar + 4 * (uint64_t)(h[0] + h[2]);
+      nq = h[0];
+      nfar = h[2];
+      lowest = h[3];
+      std::swap(far, far2);
+    }
   }
   if (st) {
     st->supersteps += steps ? steps - 1 : 0;
@@ -165,6 +406,8 @@ int gre_sssp(gre_graph g, const uint32_t* srcs, uint32_t nsrc, uint32_t* dist, g
   std::vector<uint32_t> hs(nsrc);
   if (nsrc) GRE_CUDA(cudaMemcpy(hs.data(), srcs, sizeof(uint32_t) * nsrc, cudaMemcpyDefault));
   GRE_CHECK(map_ids(g, &hs, "gre_sssp"));
+  uint32_t delta = 0;
+  GRE_CHECK(sssp_delta(g, &delta));  // before any workspace pointer is taken (it may grow WS_CUB)
   uint32_t *dfinal, *dd;
   int32_t* lv;
   GRE_CHECK(prepare_output(g, dist, (uint64_t)nsrc * n, WS_OUTBUF, &dfinal));
@@ -173,7 +416,7 @@ int gre_sssp(gre_graph g, const uint32_t* srcs, uint32_t nsrc, uint32_t* dist, g
   RunTimer timer(g);
   uint64_t edges = 0;
   for (uint32_t i = 0; i < nsrc; ++i) {
-    GRE_CHECK(sssp_one(g, hs[i], dd + (uint64_t)i * n, st, nsrc == 1));
+    GRE_CHECK(sssp_one(g, hs[i], dd + (uint64_t)i * n, st, nsrc == 1, delta));
     k_dist_to_level<<<grid_for(n, 256), 256, 0, g->stream>>>(n, dd + (uint64_t)i * n, lv);
     uint64_t e = 0;
     GRE_CHECK(count_reached_edges(g, lv, &e));

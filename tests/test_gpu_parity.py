@@ -187,6 +187,17 @@ def test_rmat14_sssp(rmat14):
     np.testing.assert_array_equal(d0, ref[0])
 
 
+@pytest.mark.parametrize("delta", [0, 1, 7, 64, 1000])
+def test_rmat14_sssp_near_far(rmat14, monkeypatch, delta):
+    """Every near-far bucket width gives the oracle's distances (0 = Bellman-Ford frontier)."""
+    n, off, col, g, R, roots = rmat14
+    g.set_weights_hash(78)
+    ref = R.sssp_many(roots, 78)
+    monkeypatch.setenv("GRE_SSSP_DELTA", str(delta))
+    d, st = G.sssp(g, roots)
+    np.testing.assert_array_equal(d.reshape(len(roots), n), ref)
+
+
 def test_rmat14_cc(rmat14):
     n, off, col, g, R, roots = rmat14
     ref, _ = R.cc()
