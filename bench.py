@@ -386,7 +386,8 @@ def run_ours(args, rank, world, local_rank):
         "per_algorithm": per_alg,
         "roofline": {"bound": "hbm", "kernel": "PageRank pull superstep (degree-binned row kernels)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "bytes_per_launch": pr_bytes_iter, "traffic": profiled_traffic()},
+                     "peak_kind": peak_kind, "bytes_per_launch": pr_bytes_iter,
+                     "traffic": profiled_traffic() if args.scale == 26 and not args.no_reorder else None},
         "batched_vs_plain": extra,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": 4, "d2h_bytes_per_step": d2h},
