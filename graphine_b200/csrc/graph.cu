@@ -10,6 +10,8 @@
 //                                                when the graph is symmetric (rarc on demand)
 //   outdeg[n] u32 (indeg[n] u32)                 degrees
 //   w32[m] u32 / w64[m] f64                      optional arc weights, CSR order
+//   perm[n], iperm[n] u32, arc_rank[m] u32       relabelled graphs only: internal <-> caller
+//                                                ids and each arc's caller position
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -185,25 +187,30 @@ __global__ void k_inverse_perm(uint64_t n, const uint32_t* __restrict__ perm, ui
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
     iperm[perm[i]] = (uint32_t)i;
 }
-__global__ void k_new_degree(uint64_t n, const uint32_t* __restrict__ perm, const uint64_t* __restrict__ off, uint64_t* __restrict__ deg) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i <= n; i += (uint64_t)gridDim.x * blockDim.x)
-    deg[i] = i < n ? off[perm[i] + 1] - off[perm[i]] : 0;
-}
-// warp per new row i: copy old row perm[i], mapping neighbour ids through `map` when given
-template <class T>
-__global__ void k_move_rows(uint64_t n, const uint32_t* __restrict__ perm, const uint64_t* __restrict__ old_off,
-                            const T* __restrict__ old_data, const uint64_t* __restrict__ new_off, T* __restrict__ new_data,
-                            const uint32_t* __restrict__ map) {
+// Relabelled arcs of caller row u (warp per row): key = new row << 32 | new column, value =
+// the arc's position in its caller row.
+__global__ void k_relabel_arcs(uint64_t n, const uint64_t* __restrict__ off, const uint32_t* __restrict__ col,
+                               const uint32_t* __restrict__ iperm, uint64_t* __restrict__ keys, uint32_t* __restrict__ rank) {
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const uint32_t lane = threadIdx.x & 31u;
-  for (uint64_t i = warp; i < n; i += nwarps) {
-    const uint64_t o0 = old_off[perm[i]], n0 = new_off[i], len = new_off[i + 1] - n0;
+  for (uint64_t u = warp; u < n; u += nwarps) {
+    const uint64_t a0 = off[u], len = off[u + 1] - a0;
+    const uint64_t hi = (uint64_t)iperm[u] << 32;
     for (uint64_t k = lane; k < len; k += 32) {
-      const T x = old_data[o0 + k];
-      new_data[n0 + k] = map ? (T)map[(uint64_t)x] : x;
+      keys[a0 + k] = hi | iperm[col[a0 + k]];
+      rank[a0 + k] = (uint32_t)k;
     }
   }
+}
+
+// out[a] = in[caller arc of internal arc a], the internal arcs sorted by (row, column) keys
+template <class T>
+__global__ void k_gather_by_rank(uint64_t m, const uint64_t* __restrict__ keys, const uint32_t* __restrict__ rank,
+                                 const uint32_t* __restrict__ perm, const uint64_t* __restrict__ coff, const T* __restrict__ in,
+                                 T* __restrict__ out) {
+  for (uint64_t a = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; a < m; a += (uint64_t)gridDim.x * blockDim.x)
+    out[a] = in[coff[perm[keys[a] >> 32]] + rank[a]];
 }
 
 __global__ void k_gather_f64(uint64_t m, const uint64_t* __restrict__ idx, const double* __restrict__ src, double* __restrict__ dst) {
@@ -310,6 +317,7 @@ static void destroy_graph(gre_graph g) {
   cudaFree(g->bc_fpool);
   cudaFree(g->perm);
   cudaFree(g->iperm);
+  cudaFree(g->arc_rank);
   g->ws.release();
   if (g->ev0) cudaEventDestroy(g->ev0);
   if (g->ev1) cudaEventDestroy(g->ev1);
@@ -439,35 +447,47 @@ static void drop_derived(gre_graph g) {
 }
 
 // Relabel by decreasing degree: new row i = old row perm[i], neighbour ids mapped through
-// iperm, arc order within a row kept; weights move with their arcs.
+// iperm, and each row's arcs sorted by new neighbour id (a stable sort: parallel arcs keep their
+// caller order).  Sorted rows put the arcs towards hubs (small new ids) side by side, so the
+// gathers of a warp share more cache lines.  Weights move with their arcs; arc_rank keeps each
+// arc's caller position for per-arc inputs and outputs.
 static int reorder_graph(gre_graph g) {
   if (g->perm) return GRE_SUCCESS;  // already relabelled
   const uint64_t n = g->n, m = g->m;
   GRE_CUDA(cudaStreamSynchronize(g->stream));
   uint32_t *k0 = nullptr, *k1 = nullptr, *v0 = nullptr, *v1 = nullptr, *perm = nullptr, *iperm = nullptr;
-  uint64_t *deg = nullptr, *noff = nullptr;
+  uint64_t *ak0 = nullptr, *ak1 = nullptr, *noff = nullptr;
+  uint32_t *av0 = nullptr, *av1 = nullptr, *rank = nullptr;
   uint32_t* ncol = nullptr;
   uint32_t* nw32 = nullptr;
   double* nw64 = nullptr;
-  auto cleanup = [&]() {
+  auto free_sort = [&]() {
     cudaFree(k0);
     cudaFree(k1);
     cudaFree(v0);
     cudaFree(v1);
-    cudaFree(deg);
+    cudaFree(ak0);
+    cudaFree(ak1);
+    k0 = k1 = v0 = v1 = nullptr;
+    ak0 = ak1 = nullptr;
   };
+  const uint64_t mm = m ? m : 1;
   cudaError_t e = cudaMalloc(&k0, 4 * n);
   if (e == cudaSuccess) e = cudaMalloc(&k1, 4 * n);
   if (e == cudaSuccess) e = cudaMalloc(&v0, 4 * n);
   if (e == cudaSuccess) e = cudaMalloc(&v1, 4 * n);
   if (e == cudaSuccess) e = cudaMalloc(&iperm, 4 * n);
-  if (e == cudaSuccess) e = cudaMalloc(&deg, 8 * (n + 1));
+  if (e == cudaSuccess) e = cudaMalloc(&ak0, 8 * mm);
+  if (e == cudaSuccess) e = cudaMalloc(&ak1, 8 * mm);
+  if (e == cudaSuccess) e = cudaMalloc(&av0, 4 * mm);
+  if (e == cudaSuccess) e = cudaMalloc(&av1, 4 * mm);
   if (e == cudaSuccess) e = cudaMalloc(&noff, 8 * (n + 1));
-  if (e == cudaSuccess) e = cudaMalloc(&ncol, 4 * (m ? m : 1));
-  if (e == cudaSuccess && g->w32) e = cudaMalloc(&nw32, 4 * (m ? m : 1));
-  if (e == cudaSuccess && g->w64) e = cudaMalloc(&nw64, 8 * (m ? m : 1));
+  if (e == cudaSuccess) e = cudaMalloc(&ncol, 4 * mm);
+  if (e == cudaSuccess && g->w32) e = cudaMalloc(&nw32, 4 * mm);
+  if (e == cudaSuccess && g->w64) e = cudaMalloc(&nw64, 8 * mm);
   int st = e == cudaSuccess ? GRE_SUCCESS : cuda_status(e, "cudaMalloc (reorder)", __FILE__, __LINE__);
   if (!st) {
+    // vertex order: stable sort by decreasing degree
     k_reorder_keys<<<grid_for(n, 256), 256, 0, g->stream>>>(n, g->off, k0, v0);
     cub::DoubleBuffer<uint32_t> dk(k0, k1), dv(v0, v1);
     size_t tb = 0;
@@ -481,26 +501,42 @@ static int reorder_graph(gre_graph g) {
     if (!st) {
       perm = dv.Current();
       k_inverse_perm<<<grid_for(n, 256), 256, 0, g->stream>>>(n, perm, iperm);
-      k_new_degree<<<grid_for(n + 1, 256), 256, 0, g->stream>>>(n, perm, g->off, deg);
-      tb = 0;
-      cub::DeviceScan::ExclusiveSum(nullptr, tb, deg, noff, n + 1, g->stream);
-      st = cub_temp(g, tb, &tmp);
-    }
-    if (!st) {
-      e = cub::DeviceScan::ExclusiveSum(tmp, tb, deg, noff, n + 1, g->stream);
-      if (e != cudaSuccess) st = cuda_status(e, "ExclusiveSum (reorder)", __FILE__, __LINE__);
-    }
-    if (!st) {
-      const int grid = grid_for(n * 32, 256);
-      k_move_rows<uint32_t><<<grid, 256, 0, g->stream>>>(n, perm, g->off, g->col, noff, ncol, iperm);
-      if (nw32) k_move_rows<uint32_t><<<grid, 256, 0, g->stream>>>(n, perm, g->off, g->w32, noff, nw32, nullptr);
-      if (nw64) k_move_rows<double><<<grid, 256, 0, g->stream>>>(n, perm, g->off, g->w64, noff, nw64, nullptr);
-      e = cudaStreamSynchronize(g->stream);
-      if (e != cudaSuccess) st = cuda_status(e, "reorder", __FILE__, __LINE__);
     }
   }
+  if (!st && m) {
+    // arcs: sort (new row, new column) keys carrying each arc's caller position
+    k_relabel_arcs<<<grid_for(n * 32, 256), 256, 0, g->stream>>>(n, g->off, g->col, iperm, ak0, av0);
+    int bits = 1;
+    while (bits < 32 && (1ull << bits) < n) ++bits;
+    cub::DoubleBuffer<uint64_t> dk(ak0, ak1);
+    cub::DoubleBuffer<uint32_t> dv(av0, av1);
+    size_t tb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, dk, dv, m, 0, 32 + bits, g->stream);
+    void* tmp = nullptr;
+    st = cub_temp(g, tb, &tmp);
+    if (!st) {
+      e = cub::DeviceRadixSort::SortPairs(tmp, tb, dk, dv, m, 0, 32 + bits, g->stream);
+      if (e != cudaSuccess) st = cuda_status(e, "SortPairs (reorder arcs)", __FILE__, __LINE__);
+    }
+    if (!st) {
+      const uint64_t* keys = dk.Current();
+      rank = dv.Current();
+      k_low32<<<grid_for(m, 256), 256, 0, g->stream>>>(m, keys, ncol);
+      k_offsets_from_sorted<<<grid_for(n + 1, 256), 256, 0, g->stream>>>(n, m, keys, noff);
+      if (nw32) k_gather_by_rank<uint32_t><<<grid_for(m, 256), 256, 0, g->stream>>>(m, keys, rank, perm, g->off, g->w32, nw32);
+      if (nw64) k_gather_by_rank<double><<<grid_for(m, 256), 256, 0, g->stream>>>(m, keys, rank, perm, g->off, g->w64, nw64);
+    }
+  } else if (!st) {
+    GRE_CUDA(cudaMemsetAsync(noff, 0, 8 * (n + 1), g->stream));
+  }
+  if (!st) {
+    e = cudaStreamSynchronize(g->stream);
+    if (e != cudaSuccess) st = cuda_status(e, "reorder", __FILE__, __LINE__);
+  }
   if (st) {
-    cleanup();
+    free_sort();
+    cudaFree(av0);
+    cudaFree(av1);
     cudaFree(iperm);
     cudaFree(noff);
     cudaFree(ncol);
@@ -508,11 +544,14 @@ static int reorder_graph(gre_graph g) {
     cudaFree(nw64);
     return st;
   }
-  // keep the sorted ids as perm; release the other sort buffers
-  uint32_t* keep = perm;
-  if (keep == v0) v0 = nullptr;
+  // keep the sorted vertex ids as perm and the sorted ranks as arc_rank; release the rest
+  if (perm == v0) v0 = nullptr;
   else v1 = nullptr;
-  cleanup();
+  if (rank == av0) av0 = nullptr;
+  else if (rank == av1) av1 = nullptr;
+  free_sort();
+  cudaFree(av0);
+  cudaFree(av1);
   drop_derived(g);
   cudaFree(g->off);
   cudaFree(g->col);
@@ -522,8 +561,9 @@ static int reorder_graph(gre_graph g) {
   g->col = ncol;
   g->w32 = nw32;
   g->w64 = nw64;
-  g->perm = keep;
+  g->perm = perm;
   g->iperm = iperm;
+  g->arc_rank = rank;
   g->h_iperm.resize(n);
   GRE_CUDA(cudaMemcpy(g->h_iperm.data(), iperm, 4 * n, cudaMemcpyDeviceToHost));
   g->flags |= GRE_GRAPH_REORDER;

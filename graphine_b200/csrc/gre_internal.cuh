@@ -116,6 +116,9 @@ struct gre_graph_s {
   uint32_t* perm = nullptr;
   uint32_t* iperm = nullptr;
   std::vector<uint32_t> h_iperm;  // host copy, to map source ids
+  // Relabelled rows are sorted by internal neighbour id; arc_rank[a] is the position of internal
+  // arc a within its caller row (caller arc = caller_off[perm[row]] + arc_rank[a]).
+  uint32_t* arc_rank = nullptr;
   gre::ChunkTable bc_chunks;       // in-arc rows longer than 512 arcs (betweenness)
   uint64_t* bc_fpool = nullptr;    // per-level frontier words of the batched betweenness
   uint64_t bc_fpool_levels = 0;

@@ -33,18 +33,20 @@ __global__ void k_caller_degree(uint64_t n, const uint32_t* __restrict__ iperm, 
     deg[v] = v < n ? off[iperm[v] + 1] - off[iperm[v]] : 0;
 }
 
-// warp per internal row i: arcs of internal row i <-> arcs of caller row perm[i]
+// warp per internal row i: arc i0 + k of internal row i <-> arc c0 + rank[i0 + k] of caller row
+// perm[i] (rows are sorted by internal neighbour id; rank is each arc's caller position)
 template <class T, bool TO_INTERNAL>
 __global__ void k_arcs(uint64_t n, const uint32_t* __restrict__ perm, const uint64_t* __restrict__ coff,
-                       const uint64_t* __restrict__ ioff, const T* __restrict__ in, T* __restrict__ out) {
+                       const uint64_t* __restrict__ ioff, const uint32_t* __restrict__ rank, const T* __restrict__ in,
+                       T* __restrict__ out) {
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const uint32_t lane = threadIdx.x & 31u;
   for (uint64_t i = warp; i < n; i += nwarps) {
     const uint64_t c0 = coff[perm[i]], i0 = ioff[i], len = ioff[i + 1] - i0;
     for (uint64_t k = lane; k < len; k += 32) {
-      if (TO_INTERNAL) out[i0 + k] = in[c0 + k];
-      else out[c0 + k] = in[i0 + k];
+      if (TO_INTERNAL) out[i0 + k] = in[c0 + rank[i0 + k]];
+      else out[c0 + rank[i0 + k]] = in[i0 + k];
     }
   }
 }
@@ -121,9 +123,11 @@ static int arcs_move(gre_graph g, const void* in_dev, void* out_dev, size_t elem
   GRE_CHECK(caller_offsets(g, &coff));
   const int grid = grid_for(g->n * 32, 256);
   if (elem == 4)
-    k_arcs<uint32_t, TO_INTERNAL><<<grid, 256, 0, g->stream>>>(g->n, g->perm, coff, g->off, (const uint32_t*)in_dev, (uint32_t*)out_dev);
+    k_arcs<uint32_t, TO_INTERNAL><<<grid, 256, 0, g->stream>>>(g->n, g->perm, coff, g->off, g->arc_rank, (const uint32_t*)in_dev,
+                                                                      (uint32_t*)out_dev);
   else if (elem == 8)
-    k_arcs<uint64_t, TO_INTERNAL><<<grid, 256, 0, g->stream>>>(g->n, g->perm, coff, g->off, (const uint64_t*)in_dev, (uint64_t*)out_dev);
+    k_arcs<uint64_t, TO_INTERNAL><<<grid, 256, 0, g->stream>>>(g->n, g->perm, coff, g->off, g->arc_rank, (const uint64_t*)in_dev,
+                                                                      (uint64_t*)out_dev);
   else return GRE_INVALID_ARG;
   GRE_LAUNCH_CHECK();
   return GRE_SUCCESS;
@@ -134,13 +138,14 @@ int arcs_to_caller(gre_graph g, const void* in_dev, void* out_dev, size_t elem) 
 
 // Caller-order CSR: row offsets and neighbour ids of caller row v = internal row iperm[v].
 __global__ void k_col_to_caller(uint64_t n, const uint32_t* __restrict__ perm, const uint64_t* __restrict__ coff,
-                                const uint64_t* __restrict__ ioff, const uint32_t* __restrict__ icol, uint32_t* __restrict__ out) {
+                                const uint64_t* __restrict__ ioff, const uint32_t* __restrict__ rank, const uint32_t* __restrict__ icol,
+                                uint32_t* __restrict__ out) {
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const uint32_t lane = threadIdx.x & 31u;
   for (uint64_t i = warp; i < n; i += nwarps) {
     const uint64_t c0 = coff[perm[i]], i0 = ioff[i], len = ioff[i + 1] - i0;
-    for (uint64_t k = lane; k < len; k += 32) out[c0 + k] = perm[icol[i0 + k]];
+    for (uint64_t k = lane; k < len; k += 32) out[c0 + rank[i0 + k]] = perm[icol[i0 + k]];
   }
 }
 
@@ -155,7 +160,7 @@ int caller_csr(gre_graph g, uint64_t* off_out, uint32_t* col_out) {
       GRE_CHECK(g->ws.get(WS_PERM_OUT, sizeof(uint32_t) * g->m, &tmp));
       dcol = (uint32_t*)tmp;
     }
-    k_col_to_caller<<<grid_for(g->n * 32, 256), 256, 0, g->stream>>>(g->n, g->perm, coff, g->off, g->col, dcol);
+    k_col_to_caller<<<grid_for(g->n * 32, 256), 256, 0, g->stream>>>(g->n, g->perm, coff, g->off, g->arc_rank, g->col, dcol);
     GRE_LAUNCH_CHECK();
     if (dcol != col_out) GRE_CUDA(cudaMemcpyAsync(col_out, dcol, sizeof(uint32_t) * g->m, cudaMemcpyDeviceToHost, g->stream));
   }

@@ -308,6 +308,52 @@ def test_graph_union_batch():
 
 
 # ---------------------------------------------------------------------------------------------
+# relabelled graphs: rows are stored sorted by internal id; per-arc data keeps the caller's order
+# ---------------------------------------------------------------------------------------------
+def _multigraph(n, m, seed):
+    """Directed multigraph in caller CSR order with parallel arcs and self loops, unsorted rows."""
+    rng = np.random.default_rng(seed)
+    src = np.minimum(rng.zipf(1.6, m) - 1, n - 1).astype(np.int64)
+    dst = rng.integers(0, n, m)
+    dst[: m // 10] = dst[m // 10: 2 * (m // 10)]  # parallel arcs
+    src[: m // 10] = src[m // 10: 2 * (m // 10)]
+    order = np.argsort(src, kind="stable")
+    src, dst = src[order], dst[order]
+    off = np.zeros(n + 1, np.uint64)
+    np.add.at(off, src + 1, 1)
+    return n, np.cumsum(off).astype(np.uint64), dst.astype(np.uint32)
+
+
+def test_relabelled_arc_order_roundtrip():
+    n, off, col = _multigraph(3000, 40000, 5)
+    g = G.Graph.from_csr(n, off, col, dir=G.InOut, reorder=True)
+    o2, c2 = g.csr()
+    np.testing.assert_array_equal(o2, off)
+    np.testing.assert_array_equal(c2, col)
+
+
+@pytest.mark.parametrize("when", ["weights_after_relabel", "weights_before_relabel"])
+def test_relabelled_explicit_weights_match_plain(when):
+    n, off, col = _multigraph(3000, 40000, 6)
+    w = np.random.default_rng(7).integers(1, 1000, len(col)).astype(np.uint32)
+    plain = G.Graph.from_csr(n, off, col, dir=G.InOut)
+    plain.loadEdgeProperty(w)
+    if when == "weights_after_relabel":
+        rel = G.Graph.from_csr(n, off, col, dir=G.InOut, reorder=True)
+        rel.loadEdgeProperty(w)
+    else:
+        rel = G.Graph.from_csr(n, off, col, dir=G.InOut)
+        rel.loadEdgeProperty(w)
+        rel.reorder()
+    roots = np.array([0, 1, 17, 2999], np.uint32)
+    d0, _ = G.sssp(plain, roots)
+    d1, _ = G.sssp(rel, roots)
+    np.testing.assert_array_equal(d1, d0)
+    d2, _, _ = G.vc_sssp(rel, 17)
+    np.testing.assert_array_equal(d2, d0.reshape(len(roots), n)[2])
+
+
+# ---------------------------------------------------------------------------------------------
 # scale 20: size-independent properties
 # ---------------------------------------------------------------------------------------------
 @pytest.fixture(scope="module")
