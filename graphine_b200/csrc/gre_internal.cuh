@@ -207,6 +207,46 @@ struct RunTimer {
   }
 };
 
+void launch_count_add(long long k);
+
+// A fixed sequence of launches on one stream, recorded once into a CUDA graph and replayed:
+// one host call per replay instead of one per kernel (supersteps whose shape does not depend
+// on data, e.g. a period of PageRank iterations).  The body may only enqueue work on the
+// stream (kernels, memsets, device-to-device copies): no allocation, no host synchronisation.
+class Recorded {
+ public:
+  Recorded() = default;
+  Recorded(const Recorded&) = delete;
+  Recorded& operator=(const Recorded&) = delete;
+  ~Recorded() {
+    if (exec_) cudaGraphExecDestroy(exec_);
+    if (graph_) cudaGraphDestroy(graph_);
+  }
+  template <class F>
+  int record(cudaStream_t s, F&& body) {
+    const unsigned long long before = gre_launch_count();
+    GRE_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    const int st = body();
+    const cudaError_t e = cudaStreamEndCapture(s, &graph_);
+    kernels_ = (long long)(gre_launch_count() - before);
+    launch_count_add(-kernels_);
+    if (st) return st;
+    GRE_CUDA(e);
+    GRE_CUDA(cudaGraphInstantiate(&exec_, graph_, 0));
+    return GRE_SUCCESS;
+  }
+  int replay(cudaStream_t s) {
+    GRE_CUDA(cudaGraphLaunch(exec_, s));
+    launch_count_add(kernels_);
+    return GRE_SUCCESS;
+  }
+
+ private:
+  cudaGraph_t graph_ = nullptr;
+  cudaGraphExec_t exec_ = nullptr;
+  long long kernels_ = 0;
+};
+
 inline void stats_reset(gre_stats* st) {
   if (!st) return;
   st->supersteps = 0;

@@ -23,3 +23,10 @@ cudaError_t __wrap_cudaLaunchKernel(const void* func, dim3 grid, dim3 block, voi
 uint64_t gre_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 }  // extern "C"
+
+namespace gre {
+// Kernels run from a CUDA graph do not pass through cudaLaunchKernel: a recorded sequence takes
+// back the launches counted while it was captured (they did not run then) and adds them again
+// at every replay.
+void launch_count_add(long long k) { g_launches.fetch_add((unsigned long long)k, std::memory_order_relaxed); }
+}  // namespace gre

@@ -15,6 +15,7 @@
 // HBM bytes per superstep (algorithmic): 8(n+1) offsets + 4m columns + 8m gathered contrib
 // + 4n outdeg + 16n (pr and contrib writes) = 8(n+1) + 12m + 20n.
 #include <algorithm>
+#include <memory>
 
 #include "gre_internal.cuh"
 #include "rows.cuh"
@@ -412,17 +413,34 @@ static int affine_solve(gre_graph g, const DegreeBins& B, const uint64_t* off, c
   GRE_CHECK(ws_array(g, WS_H, B.n_hub_chunks + 1, &partial));
   GRE_CHECK(ws_array(g, WS_COUNTERS, 2, &maxdiff));
   k_affine_init<<<grid_for(g->n, 256), 256, 0, g->stream>>>(g->n, base, base_c, scale, xa, xb);
+  // one iteration x -> y; maxdiff holds that iteration's largest change (reset first)
+  auto iteration = [&](double* x, double* y) -> int {
+    GRE_CUDA(cudaMemsetAsync(maxdiff, 0, sizeof(double), g->stream));
+    // rows without arcs keep base (set by init in both buffers)
+    return rows::reduce_rows(B, off, GatherWeighted{col, p, x}, FinishAffine{y, x, base, base_c, scale, d, maxdiff}, partial,
+                             g->stream);
+  };
+  // convergence is read every check_every iterations (an even number: the buffers are back in
+  // place), so that block is recorded once as a CUDA graph and replayed until it converges
+  const uint32_t check_every = 4;
+  Recorded rec;
+  GRE_CHECK(rec.record(g->stream, [&]() {
+    int e = 0;
+    for (uint32_t i = 0; i < check_every && !e; ++i) e = (i & 1) ? iteration(xb, xa) : iteration(xa, xb);
+    return e;
+  }));
   double* x = xa;
   double* y = xb;
   uint32_t it = 0;
-  const uint32_t check_every = 4;
-  for (it = 0; it < max_iters;) {
-    GRE_CUDA(cudaMemsetAsync(maxdiff, 0, sizeof(double), g->stream));
-    // rows without arcs keep base (set by init in both buffers)
-    GRE_CHECK(rows::reduce_rows(B, off, GatherWeighted{col, p, x}, FinishAffine{y, x, base, base_c, scale, d, maxdiff}, partial,
-                                g->stream));
-    std::swap(x, y);
-    ++it;
+  while (it < max_iters) {
+    if (it + check_every <= max_iters && x == xa) {
+      GRE_CHECK(rec.replay(g->stream));
+      it += check_every;
+    } else {
+      GRE_CHECK(iteration(x, y));
+      std::swap(x, y);
+      ++it;
+    }
     if (it % check_every == 0 || it == max_iters) {
       double h = 0;
       GRE_CUDA(cudaMemcpyAsync(&h, maxdiff, sizeof h, cudaMemcpyDeviceToHost, g->stream));
@@ -459,11 +477,26 @@ int gre_pagerank(gre_graph g, int variant, double d, uint32_t iters, double* pr,
   RunTimer timer(g);
   k_pr_init<<<grid_for(n, 256), 256, 0, g->stream>>>(n, g->outdeg, tele, dpr, c0, refresh ? c1 : nullptr);
   GRE_LAUNCH_CHECK();
-  double* cur = c0;
-  double* nxt = c1;
-  for (uint32_t it = 0; it < iters; ++it) {
-    FinishPR fin{dpr, refresh ? nxt : nullptr, g->outdeg, tele, d};
-    GRE_CHECK(rows::reduce_rows(g->bins_in, g->roff, GatherContrib{g->rcol, cur}, fin, partial, g->stream));
+  // one superstep reads contributions `a` and (power iteration) writes the next ones to `b`
+  auto superstep = [&](double* a, double* b) -> int {
+    FinishPR fin{dpr, refresh ? b : nullptr, g->outdeg, tele, d};
+    return rows::reduce_rows(g->bins_in, g->roff, GatherContrib{g->rcol, a}, fin, partial, g->stream);
+  };
+  // supersteps repeat with period 2 (the contribution buffers swap), 1 for the reference
+  // variant: that period is recorded once as a CUDA graph and replayed
+  const uint32_t period = refresh ? 2 : 1;
+  uint32_t done = 0;
+  if (iters >= 2 * period) {
+    Recorded rec;
+    GRE_CHECK(rec.record(g->stream, [&]() {
+      int e = superstep(c0, c1);
+      if (!e && refresh) e = superstep(c1, c0);
+      return e;
+    }));
+    for (; done + period <= iters; done += period) GRE_CHECK(rec.replay(g->stream));
+  }
+  for (double *cur = c0, *nxt = c1; done < iters; ++done) {
+    GRE_CHECK(superstep(cur, nxt));
     if (refresh) std::swap(cur, nxt);
   }
   GRE_CHECK(perm_out_end(g, dpr, dout, 1, 8));
@@ -525,24 +558,37 @@ int gre_ppr(gre_graph g, const uint32_t* seeds, uint32_t k, double d, uint32_t i
     const DegreeBins& B = g->bins_in;
     uint64_t short_rows = 0;
     for (int b = 0; b < 6; ++b) short_rows += B.count[b];  // rows longer than kPprChunk are skipped
+    std::unique_ptr<Recorded> rec;
+    uint32_t rec_kk = 0;
     for (uint32_t j0 = 0; j0 < k; j0 += kCols) {
       const uint32_t kk = (k - j0) < (uint32_t)kCols ? (k - j0) : (uint32_t)kCols;
       GRE_CUDA(cudaMemcpyAsync(dseeds, hs.data() + j0, sizeof(uint32_t) * kk, cudaMemcpyHostToDevice, g->stream));
       k_ppr_init<<<grid_for(n * kCols, 256), 256, 0, g->stream>>>(n, kk, dseeds, g->outdeg, tele, x, c0, c1);
       k_ppr_seed<<<1, 128, 0, g->stream>>>(kk, dseeds, g->outdeg, tele, x, c0, c1);
-      double* cur = c0;
-      double* nxt = c1;
-      for (uint32_t it = 0; it < iters; ++it) {
-        PprRow R{g->roff, g->rcol, cur};
-        PprFinish F{x, nxt, g->outdeg, dseeds, kk, tele, d};
+      auto superstep = [&](double* a, double* b) -> int {
+        PprRow R{g->roff, g->rcol, a};
+        PprFinish F{x, b, g->outdeg, dseeds, kk, tele, d};
         if (short_rows) k_ppr_rows<<<grid_for(short_rows * 32, 256, 8), 256, 0, g->stream>>>(B.rows, short_rows, R, F);
         if (pc.nrows) {
           k_ppr_chunks<<<grid_for(pc.nchunks * 32, 256, 8), 256, 0, g->stream>>>(pc.rows, pc.row, pc.begin, pc.nchunks, R, partial);
           k_ppr_chunk_finish<<<grid_for(pc.nrows * 32, 256, 8), 256, 0, g->stream>>>(pc.rows, pc.nrows, pc.first, partial, F);
         }
         GRE_LAUNCH_CHECK();
-        std::swap(cur, nxt);
+        return GRE_SUCCESS;
+      };
+      // two supersteps (the buffers swap back) recorded once per block width, then replayed
+      if (!rec || rec_kk != kk) {
+        rec.reset(new Recorded());
+        rec_kk = kk;
+        GRE_CHECK(rec->record(g->stream, [&]() {
+          int e = superstep(c0, c1);
+          if (!e) e = superstep(c1, c0);
+          return e;
+        }));
       }
+      uint32_t it = 0;
+      for (; it + 2 <= iters; it += 2) GRE_CHECK(rec->replay(g->stream));
+      if (it < iters) GRE_CHECK(superstep(c0, c1));
       k_ppr_transpose<<<grid_for((uint64_t)kk * n, 256), 256, 0, g->stream>>>(n, kk, x, dout + (uint64_t)j0 * n);
       GRE_LAUNCH_CHECK();
     }
