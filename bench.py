@@ -382,6 +382,7 @@ def run_ours(args, rank, world, local_rank):
         "config": {"workload": f"GRE plain suite on RMAT scale {args.scale} EF16 symmetric: PageRank-{PR_ITERS} (power "
                                f"iteration, FP64), DO-BFS 1 src, SSSP 1 src (u32 w in [1,255]), CC",
                    "graph_n": n, "graph_arcs": m, "parallelism": f"replica x{world}",
+                   "row_schedule": dict(zip(("lane_arcs", "cta_min", "hub_chunk"), g.row_schedule(True))),
                    "l2": "inputs larger than L2 (graph > 126 MB)"},
         "per_algorithm": per_alg,
         "roofline": {"bound": "hbm", "kernel": "PageRank pull superstep (degree-binned row kernels)",

@@ -227,36 +227,6 @@ __global__ void k_shift_u32(uint64_t cnt, const uint32_t* __restrict__ in, uint3
     out[i] = in[i] + add;
 }
 
-__global__ void k_bin_of(uint64_t n, const uint64_t* __restrict__ off, uint8_t* __restrict__ bin) {
-  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t d = off[v + 1] - off[v];
-    uint8_t b;
-    // lanes per row = degree / 4 rounded up to a power of two (each lane gathers 4 arcs per
-    // pass), a CTA beyond 4096 arcs, CTA chunks beyond 65536
-    if (d == 0) b = 255;
-    else if (d <= 4) b = 0;
-    else if (d <= 8) b = 1;
-    else if (d <= 16) b = 2;
-    else if (d <= 32) b = 3;
-    else if (d <= 64) b = 4;
-    else if (d <= 4096) b = 5;
-    else if (d <= 65536) b = 6;
-    else b = 7;
-    bin[v] = b;
-  }
-}
-
-struct BinIs {
-  const uint8_t* bin;
-  uint8_t b;
-  __host__ __device__ __forceinline__ bool operator()(const uint32_t& v) const { return bin[v] == b; }
-};
-
-__global__ void k_iota(uint64_t n, uint32_t* __restrict__ out) {
-  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x)
-    out[v] = (uint32_t)v;
-}
-
 // ---------------------------------------------------------------------------------------------
 // construction helpers
 // ---------------------------------------------------------------------------------------------
@@ -635,84 +605,6 @@ int ensure_rarc(gre_graph g) {
     g->rcol = g->col;
     g->rarc = nullptr;
   }
-  return st;
-}
-
-int ensure_bins(gre_graph g, bool in) {
-  DegreeBins& B = in ? g->bins_in : g->bins_out;
-  if (B.ready) return GRE_SUCCESS;
-  const uint64_t n = g->n;
-  const uint64_t* off = in ? g->roff : g->off;
-  uint8_t* bin = nullptr;
-  uint32_t* iota = nullptr;
-  uint64_t* nsel = nullptr;
-  GRE_CUDA(cudaMalloc(&bin, n));
-  cudaError_t e = cudaMalloc(&iota, sizeof(uint32_t) * n);
-  if (e == cudaSuccess) e = cudaMalloc(&nsel, sizeof(uint64_t) * DegreeBins::NB);
-  if (e == cudaSuccess) e = cudaMalloc(&B.rows, sizeof(uint32_t) * (n ? n : 1));
-  int st = e == cudaSuccess ? GRE_SUCCESS : cuda_status(e, "cudaMalloc (bins)", __FILE__, __LINE__);
-  if (!st) {
-    k_bin_of<<<grid_for(n, 256), 256, 0, g->stream>>>(n, off, bin);
-    k_iota<<<grid_for(n, 256), 256, 0, g->stream>>>(n, iota);
-    uint64_t base = 0;
-    for (int b = 0; b < DegreeBins::NB && !st; ++b) {
-      size_t tb = 0;
-      BinIs pred{bin, (uint8_t)b};
-      cub::DeviceSelect::If(nullptr, tb, iota, B.rows + base, nsel + b, n, pred, g->stream);
-      void* tmp = nullptr;
-      st = cub_temp(g, tb, &tmp);
-      if (st) break;
-      e = cub::DeviceSelect::If(tmp, tb, iota, B.rows + base, nsel + b, n, pred, g->stream);
-      if (e != cudaSuccess) {
-        st = cuda_status(e, "DeviceSelect::If", __FILE__, __LINE__);
-        break;
-      }
-      uint64_t cnt = 0;
-      e = cudaMemcpyAsync(&cnt, nsel + b, sizeof cnt, cudaMemcpyDeviceToHost, g->stream);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
-      if (e != cudaSuccess) {
-        st = cuda_status(e, "bin count", __FILE__, __LINE__);
-        break;
-      }
-      B.start[b] = base;
-      B.count[b] = cnt;
-      base += cnt;
-    }
-  }
-  // chunks of the multi-CTA bin (rows with more than 65536 arcs)
-  if (!st && B.count[7]) {
-    const uint64_t cnt = B.count[7];
-    std::vector<uint32_t> rows(cnt);
-    std::vector<uint64_t> ho(n + 1);
-    e = cudaMemcpy(rows.data(), B.rows + B.start[7], sizeof(uint32_t) * cnt, cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess) e = cudaMemcpy(ho.data(), off, sizeof(uint64_t) * (n + 1), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) st = cuda_status(e, "hub chunks", __FILE__, __LINE__);
-    if (!st) {
-      const uint64_t CH = 65536;
-      std::vector<uint64_t> crow, cbeg, first;
-      for (uint64_t i = 0; i < cnt; ++i) {
-        first.push_back(crow.size());
-        const uint64_t a0 = ho[rows[i]], a1 = ho[rows[i] + 1];
-        for (uint64_t a = a0; a < a1; a += CH) {
-          crow.push_back(i);
-          cbeg.push_back(a);
-        }
-      }
-      first.push_back(crow.size());
-      B.n_hub_chunks = crow.size();
-      e = cudaMalloc(&B.hub_chunk_row, sizeof(uint64_t) * crow.size());
-      if (e == cudaSuccess) e = cudaMalloc(&B.hub_chunk_begin, sizeof(uint64_t) * cbeg.size());
-      if (e == cudaSuccess) e = cudaMalloc(&B.hub_chunk_first, sizeof(uint64_t) * first.size());
-      if (e == cudaSuccess) e = cudaMemcpy(B.hub_chunk_row, crow.data(), sizeof(uint64_t) * crow.size(), cudaMemcpyHostToDevice);
-      if (e == cudaSuccess) e = cudaMemcpy(B.hub_chunk_begin, cbeg.data(), sizeof(uint64_t) * cbeg.size(), cudaMemcpyHostToDevice);
-      if (e == cudaSuccess) e = cudaMemcpy(B.hub_chunk_first, first.data(), sizeof(uint64_t) * first.size(), cudaMemcpyHostToDevice);
-      if (e != cudaSuccess) st = cuda_status(e, "hub chunk upload", __FILE__, __LINE__);
-    }
-  }
-  cudaFree(bin);
-  cudaFree(iota);
-  cudaFree(nsel);
-  if (!st) B.ready = true;
   return st;
 }
 

@@ -61,8 +61,19 @@ struct Workspace {
 };
 
 // Degree bins of one adjacency (rows grouped by the number of lanes that process them).
+// Threads-per-row schedule of the degree bins: bin b < 5 (2^b lanes per row) takes rows of up to
+// lane_arcs * 2^b arcs, bin 5 (a warp) rows up to cta_min arcs, bin 6 (a CTA) rows up to
+// hub_chunk arcs, bin 7 the longer rows in chunks of hub_chunk arcs.  Chosen per graph by the
+// autotuner (bins.cu) from the degree distribution.
+struct RowSchedule {
+  uint32_t lane_arcs = 4;
+  uint64_t cta_min = 4096;
+  uint64_t hub_chunk = 65536;
+};
+
 struct DegreeBins {
   bool ready = false;
+  RowSchedule sched;
   static const int NB = 8;  // 1,2,4,8,16,32 lanes, CTA per row, multi-CTA per row
   uint64_t count[NB] = {};
   uint64_t start[NB] = {};   // offsets into `rows`

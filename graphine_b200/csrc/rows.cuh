@@ -1,12 +1,13 @@
 // Degree-binned row reductions over a CSR or CSC: the pull form of the superstep's
 // scatter+combine for sums (PageRank, weighted PageRank, its adjoint).
 //
-// Rows are grouped once per graph by degree (DegreeBins): bins 0..5 give a row 1, 2, 4, 8, 16
-// or 32 lanes (degree 1-4, 5-8, 9-16, 17-32, 33-64, 65-4096: about four arcs per lane per
-// pass); bin 6 gives a row one CTA (4097-65536); bin 7 splits a row into chunks of 65536 arcs,
-// one CTA each, whose partial sums are added in chunk order by a second kernel.  Lane j of a
-// group adds arcs j, j+L, j+2L, ... (four independent loads per pass) and the group reduces
-// with xor shuffles, so every row's sum has a fixed association order: results are
+// Rows are grouped once per graph by degree (DegreeBins, schedule chosen by the autotuner in
+// bins.cu): bins 0..5 give a row 1, 2, 4, 8, 16 or 32 lanes (by default degree 1-4, 5-8, 9-16,
+// 17-32, 33-64, 65-4096: about four arcs per lane per pass); bin 6 gives a row one CTA (by
+// default 4097-65536); bin 7 splits a row into chunks of hub_chunk arcs (65536), one CTA each,
+// whose partial sums are added in chunk order by a second kernel.  Lane j of a group adds arcs
+// j, j+L, j+2L, ... (four independent loads per pass) and the group reduces with xor shuffles,
+// so every row's sum has a fixed association order for a given schedule: results are
 // deterministic run to run.  Column indices of one group are contiguous (coalesced); the
 // gathered value is the only random access.
 //
@@ -19,7 +20,6 @@ namespace gre {
 namespace rows {
 
 constexpr int kCta = 256;
-constexpr uint64_t kHubChunk = 65536;
 
 // Sum of gat(v, a) over a = a0 + lig, a0 + lig + L, ... < a1.  Four arcs per pass so that each
 // lane has four independent (column, gathered value) load chains in flight: the loop is bound
@@ -91,14 +91,14 @@ __global__ void __launch_bounds__(kCta) k_rows_cta(const uint32_t* __restrict__ 
 
 template <class Gather>
 __global__ void __launch_bounds__(kCta) k_rows_chunks(const uint32_t* __restrict__ rows, const uint64_t* __restrict__ chunk_row,
-                                                       const uint64_t* __restrict__ chunk_begin, uint64_t nchunks,
+                                                       const uint64_t* __restrict__ chunk_begin, uint64_t nchunks, uint64_t chunk,
                                                        const uint64_t* __restrict__ off, Gather gat, double* __restrict__ partial) {
   __shared__ double smem[kCta / 32];
   for (uint64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
     const uint32_t v = rows[chunk_row[c]];
     const uint64_t a0 = chunk_begin[c];
     const uint64_t end = off[v + 1];
-    const uint64_t a1 = (a0 + kHubChunk < end) ? a0 + kHubChunk : end;
+    const uint64_t a1 = (a0 + chunk < end) ? a0 + chunk : end;
     double acc = strided_sum<kCta>(gat, v, a0, a1, threadIdx.x);
     acc = block_sum(acc, smem);
     if (threadIdx.x == 0) partial[c] = acc;
@@ -129,7 +129,7 @@ int reduce_rows(const DegreeBins& B, const uint64_t* off, Gather gat, Finish fin
   if (B.count[6]) k_rows_cta<<<grid_for(B.count[6] * kCta, kCta, 8), kCta, 0, s>>>(r + B.start[6], B.count[6], off, gat, fin);
   if (B.count[7]) {
     k_rows_chunks<<<grid_for(B.n_hub_chunks * kCta, kCta, 8), kCta, 0, s>>>(r + B.start[7], B.hub_chunk_row, B.hub_chunk_begin,
-                                                                            B.n_hub_chunks, off, gat, partial);
+                                                                            B.n_hub_chunks, B.sched.hub_chunk, off, gat, partial);
     k_rows_chunk_finish<<<grid_for(B.count[7], 128, 4), 128, 0, s>>>(r + B.start[7], B.count[7], B.hub_chunk_first, partial, fin);
   }
   GRE_LAUNCH_CHECK();

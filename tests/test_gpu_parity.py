@@ -353,6 +353,24 @@ def test_relabelled_explicit_weights_match_plain(when):
     np.testing.assert_array_equal(d2, d0.reshape(len(roots), n)[2])
 
 
+def test_autotuned_row_schedule_keeps_results(monkeypatch):
+    """The tuner picks a schedule from its candidates; results equal the default schedule's
+    (bit-exact for BFS/CC, FP64 sums within a few ulps: only the association order differs)."""
+    g = G.Graph.rmat(20, 16, 77, True, reorder=True)
+    lane_arcs, cta_min, hub = g.row_schedule()
+    assert lane_arcs in (2, 4, 8) and cta_min in (1024, 4096, 16384) and hub == 65536
+    monkeypatch.setenv("GRE_TUNE", "0")
+    g0 = G.Graph.rmat(20, 16, 77, True, reorder=True)
+    assert g0.row_schedule() == (4, 4096, 65536)
+    pr, _ = G.pagerank(g, G.PR_ITER, 0.85, 20)
+    pr0, _ = G.pagerank(g0, G.PR_ITER, 0.85, 20)
+    assert rel_l1(pr, pr0) <= 1e-13
+    off, _ = g.csr()
+    roots = G.sample_sources(off, 64, 3)
+    np.testing.assert_array_equal(G.msbfs(g, roots)[0], G.msbfs(g0, roots)[0])
+    np.testing.assert_array_equal(G.cc(g)[0], G.cc(g0)[0])
+
+
 # ---------------------------------------------------------------------------------------------
 # scale 20: size-independent properties
 # ---------------------------------------------------------------------------------------------
