@@ -230,7 +230,7 @@ __global__ void k_shift_u32(uint64_t cnt, const uint32_t* __restrict__ in, uint3
 // ---------------------------------------------------------------------------------------------
 // construction helpers
 // ---------------------------------------------------------------------------------------------
-static int new_graph(int device, uint32_t flags, gre_graph* out) {
+int new_graph(int device, uint32_t flags, gre_graph* out) {
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess || ndev == 0) {
@@ -257,7 +257,7 @@ static int new_graph(int device, uint32_t flags, gre_graph* out) {
   return GRE_SUCCESS;
 }
 
-static void destroy_graph(gre_graph g) {
+void destroy_graph(gre_graph g) {
   if (!g) return;
   cudaSetDevice(g->device);
   if (g->stream) cudaStreamSynchronize(g->stream);
@@ -295,17 +295,6 @@ static void destroy_graph(gre_graph g) {
   delete g;
 }
 
-struct GraphGuard {
-  gre_graph g;
-  ~GraphGuard() {
-    if (g) destroy_graph(g);
-  }
-  gre_graph release() {
-    gre_graph r = g;
-    g = nullptr;
-    return r;
-  }
-};
 
 static int cub_temp(gre_graph g, size_t bytes, void** p) { return g->ws.get(WS_CUB, bytes, p); }
 
@@ -354,7 +343,7 @@ static int build_csc(gre_graph g) {
 }
 
 // Degrees, maxima and the CSC; called once the CSR is on the device.
-static int finish_graph(gre_graph g) {
+int finish_graph(gre_graph g) {
   const uint64_t n = g->n;
   GRE_CUDA(cudaMalloc(&g->outdeg, sizeof(uint32_t) * n));
   k_degree<<<grid_for(n, 256), 256, 0, g->stream>>>(n, g->off, g->outdeg);
@@ -421,7 +410,7 @@ static void drop_derived(gre_graph g) {
 // caller order).  Sorted rows put the arcs towards hubs (small new ids) side by side, so the
 // gathers of a warp share more cache lines.  Weights move with their arcs; arc_rank keeps each
 // arc's caller position for per-arc inputs and outputs.
-static int reorder_graph(gre_graph g) {
+int reorder_graph(gre_graph g) {
   if (g->perm) return GRE_SUCCESS;  // already relabelled
   const uint64_t n = g->n, m = g->m;
   GRE_CUDA(cudaStreamSynchronize(g->stream));
@@ -641,16 +630,7 @@ int gre_device_count(int* count) {
 int gre_graph_load(const char* prefix, uint32_t flags, int device, gre_graph* out) {
   if (!prefix || !out) return GRE_NULL;
   clear_error();
-  HostEdges e;
-  int st = host_read_edgelists(prefix, &e);
-  if (st) {
-    set_error("failed to read %s.meta / %s.edges.<i>: %s", prefix, prefix, gre_status_str(st));
-    return st;
-  }
-  std::vector<uint64_t> off;
-  std::vector<uint32_t> col;
-  host_build_csr(e.n, e.src, e.dst, false, &off, &col);
-  return make_from_host_csr(e.n, col.size(), off.data(), col.data(), flags, device, out);
+  return device_ingest(prefix, flags, device, out);
 }
 
 int gre_graph_from_edges(uint64_t n, uint64_t m, const uint32_t* src, const uint32_t* dst, uint32_t flags, int device,

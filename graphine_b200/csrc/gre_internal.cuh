@@ -218,6 +218,27 @@ struct RunTimer {
   }
 };
 
+// Graph construction steps (graph.cu): an empty handle on `device`; degrees, maxima and CSC once
+// off/col are on the device; degree-ordered relabelling with sorted rows; teardown.
+int new_graph(int device, uint32_t flags, gre_graph* out);
+int finish_graph(gre_graph g);
+int reorder_graph(gre_graph g);
+void destroy_graph(gre_graph g);
+// Frees a half-built handle on an error path unless released.
+struct GraphGuard {
+  gre_graph g;
+  ~GraphGuard() {
+    if (g) destroy_graph(g);
+  }
+  gre_graph release() {
+    gre_graph r = g;
+    g = nullptr;
+    return r;
+  }
+};
+// <prefix>.meta + <prefix>.edges.<i> parsed on the device (ingest.cu).
+int device_ingest(const char* prefix, uint32_t flags, int device, gre_graph* out);
+
 void launch_count_add(long long k);
 
 // A fixed sequence of launches on one stream, recorded once into a CUDA graph and replayed:

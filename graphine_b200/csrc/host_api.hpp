@@ -12,18 +12,10 @@ struct HostCSR {
   std::vector<uint32_t> col;
 };
 
-struct HostEdges {
-  uint64_t n = 0;       // vertex count from .meta
-  uint64_t meta_m = 0;  // edge count from .meta (informational, as in the reference)
-  std::vector<uint32_t> src, dst;
-};
-
 int host_rmat_csr(uint32_t scale, uint32_t edgefactor, uint64_t seed, int symmetric, HostCSR* out);
 int host_write_edgelists(const char* prefix, uint64_t n, uint64_t m, const uint64_t* off,
                          const uint32_t* col, uint32_t nfiles);
 int host_write_roots(const char* prefix, const uint32_t* roots, uint32_t count);
-int host_read_meta(const char* prefix, uint64_t* nv, uint64_t* ne);
-int host_read_edgelists(const char* prefix, HostEdges* out);
 int host_read_roots(const char* prefix, std::vector<uint32_t>* roots);
 void host_build_csr(uint64_t n, const std::vector<uint32_t>& src, const std::vector<uint32_t>& dst,
                     bool by_dst, std::vector<uint64_t>* off, std::vector<uint32_t>* col);

@@ -139,127 +139,6 @@ int host_write_roots(const char* prefix, const uint32_t* roots, uint32_t count) 
   return fclose(f) == 0 ? GRE_SUCCESS : GRE_IO_ERROR;
 }
 
-// ---------------------------------------------------------------------------------------------
-// Text loader.  Each file is read whole and parsed in parallel chunks that start at line
-// boundaries; chunk results are concatenated in file order, so the edge order equals the
-// order a single reader would see (the order GraphInCSR::build preserves).
-// ---------------------------------------------------------------------------------------------
-static bool read_file(const std::string& name, std::vector<char>* data) {
-  FILE* f = fopen(name.c_str(), "rb");
-  if (!f) return false;
-  fseek(f, 0, SEEK_END);
-  long sz = ftell(f);
-  fseek(f, 0, SEEK_SET);
-  data->resize((size_t)(sz > 0 ? sz : 0) + 1);
-  size_t got = sz > 0 ? fread(data->data(), 1, (size_t)sz, f) : 0;
-  fclose(f);
-  data->resize(got);
-  data->push_back('\n');  // a last line without newline is still a line (std::getline)
-  return true;
-}
-
-// Parses one chunk [b, e) of whole lines.  Returns false on a malformed line.
-static bool parse_chunk(const char* b, const char* e, std::vector<uint32_t>* src,
-                        std::vector<uint32_t>* dst, uint64_t nv, int* err) {
-  const char* p = b;
-  while (p < e) {
-    const char* eol = (const char*)memchr(p, '\n', (size_t)(e - p));
-    if (!eol) eol = e;
-    const char* q = p;
-    // skip a trailing '\r' (files written on other systems)
-    const char* lend = (eol > p && eol[-1] == '\r') ? eol - 1 : eol;
-    if (lend == p || *p == '#') {
-      p = eol + 1;
-      continue;
-    }
-    uint64_t vals[2];
-    for (int k = 0; k < 2; ++k) {
-      while (q < lend && (*q == ' ' || *q == '\t')) ++q;
-      if (q >= lend || *q < '0' || *q > '9') {
-        *err = GRE_IO_ERROR;
-        return false;
-      }
-      uint64_t x = 0;
-      while (q < lend && *q >= '0' && *q <= '9') {
-        x = x * 10 + (uint64_t)(*q - '0');
-        if (x > 0xffffffffull) {
-          *err = GRE_INVALID_ARG;
-          return false;
-        }
-        ++q;
-      }
-      vals[k] = x;
-    }
-    while (q < lend && (*q == ' ' || *q == '\t')) ++q;
-    if (q != lend) {  // extra tokens (e.g. a weight column) are not part of this format
-      *err = GRE_IO_ERROR;
-      return false;
-    }
-    if (vals[0] >= nv || vals[1] >= nv) {
-      *err = GRE_INVALID_ARG;
-      return false;
-    }
-    src->push_back((uint32_t)vals[0]);
-    dst->push_back((uint32_t)vals[1]);
-    p = eol + 1;
-  }
-  return true;
-}
-
-int host_read_meta(const char* prefix, uint64_t* nv, uint64_t* ne) {
-  std::string name = std::string(prefix) + ".meta";
-  FILE* f = fopen(name.c_str(), "r");
-  if (!f) return GRE_IO_ERROR;
-  unsigned long long a = 0, b = 0;
-  int k = fscanf(f, "%llu %llu", &a, &b);
-  fclose(f);
-  if (k != 2) return GRE_IO_ERROR;
-  if (a == 0 || a > 0xffffffffull) return GRE_INVALID_ARG;
-  *nv = a;
-  *ne = b;
-  return GRE_SUCCESS;
-}
-
-int host_read_edgelists(const char* prefix, HostEdges* out) {
-  if (!prefix) return GRE_NULL;
-  uint64_t nv = 0, ne = 0;
-  int st = host_read_meta(prefix, &nv, &ne);
-  if (st) return st;
-  out->n = nv;
-  out->meta_m = ne;
-  out->src.clear();
-  out->dst.clear();
-  for (int i = 0;; ++i) {
-    std::vector<char> data;
-    if (!read_file(std::string(prefix) + ".edges." + std::to_string(i), &data)) {
-      if (i == 0) return GRE_IO_ERROR;  // no edge file at all
-      break;
-    }
-    const int nchunks = std::max(1, std::min<int>(omp_get_max_threads() * 4,
-                                                  (int)(data.size() >> 20) + 1));
-    std::vector<size_t> cut(nchunks + 1, data.size());
-    cut[0] = 0;
-    for (int c = 1; c < nchunks; ++c) {
-      size_t pos = data.size() * (size_t)c / (size_t)nchunks;
-      if (pos < cut[c - 1]) pos = cut[c - 1];
-      const char* nl = (const char*)memchr(data.data() + pos, '\n', data.size() - pos);
-      cut[c] = nl ? (size_t)(nl - data.data()) + 1 : data.size();
-    }
-    std::vector<std::vector<uint32_t>> cs(nchunks), cd(nchunks);
-    std::vector<int> errs(nchunks, 0);
-#pragma omp parallel for schedule(dynamic, 1)
-    for (int c = 0; c < nchunks; ++c)
-      parse_chunk(data.data() + cut[c], data.data() + cut[c + 1], &cs[c], &cd[c], nv, &errs[c]);
-    for (int c = 0; c < nchunks; ++c)
-      if (errs[c]) return errs[c];
-    for (int c = 0; c < nchunks; ++c) {
-      out->src.insert(out->src.end(), cs[c].begin(), cs[c].end());
-      out->dst.insert(out->dst.end(), cd[c].begin(), cd[c].end());
-    }
-  }
-  return GRE_SUCCESS;
-}
-
 int host_read_roots(const char* prefix, std::vector<uint32_t>* roots) {
   std::string name = std::string(prefix) + ".roots";
   FILE* f = fopen(name.c_str(), "r");

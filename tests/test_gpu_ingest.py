@@ -1,0 +1,121 @@
+"""Device-side ingress (graphine_b200/csrc/ingest.cu): <prefix>.meta + <prefix>.edges.<i> parsed
+on the GPU must give the CSR a line-by-line reader gives (file order within a source, files in
+index order) and the same error codes, including when lines straddle the streaming chunks."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import graphine_b200.gre as G
+
+pytestmark = pytest.mark.gpu
+
+
+def reader_csr(n, texts):
+    """The loader's rules, line by line: blank and '#' lines skipped, a trailing CR ignored."""
+    src, dst = [], []
+    for t in texts:
+        for line in t.split("\n"):
+            line = line[:-1] if line.endswith("\r") else line
+            if not line or line[0] == "#":
+                continue
+            u, v = line.split()
+            src.append(int(u))
+            dst.append(int(v))
+    order = np.argsort(np.array(src, dtype=np.int64), kind="stable")
+    off = np.zeros(n + 1, np.uint64)
+    np.add.at(off, np.array(src, dtype=np.int64) + 1, 1)
+    return np.cumsum(off).astype(np.uint64), np.array(dst, dtype=np.uint32)[order]
+
+
+def write(td, n, texts):
+    p = os.path.join(td, "g")
+    open(p + ".meta", "w").write(f"{n} 0\n")
+    for i, t in enumerate(texts):
+        open(p + f".edges.{i}", "w", newline="").write(t)
+    return p
+
+
+def messy_texts(n, seed):
+    rng = np.random.default_rng(seed)
+    texts = []
+    for f in range(3):
+        lines = []
+        for _ in range(int(rng.integers(200, 400))):
+            r = rng.random()
+            if r < 0.05:
+                lines.append("# a comment 1 2")
+            elif r < 0.08:
+                lines.append("")
+            else:
+                u, v = rng.integers(0, n, 2)
+                sep = " " * int(rng.integers(1, 4)) if rng.random() < 0.8 else "\t"
+                lead = " " if rng.random() < 0.1 else ""
+                tail = "\r" if rng.random() < 0.1 else (" " if rng.random() < 0.1 else "")
+                lines.append(f"{lead}{u}{sep}{v}{tail}")
+        t = "\n".join(lines)
+        texts.append(t if f == 1 else t + "\n")  # file 1 ends without a newline
+    return texts
+
+
+@pytest.mark.parametrize("chunk", [None, "64", "100", "4096"])
+def test_device_parse_matches_line_reader(monkeypatch, chunk):
+    if chunk:
+        monkeypatch.setenv("GRE_INGEST_CHUNK", chunk)
+    n = 500
+    texts = messy_texts(n, 3)
+    with tempfile.TemporaryDirectory() as td:
+        g = G.Graph.ingress(write(td, n, texts), G.InOut)
+    off, col = g.csr()
+    ref_off, ref_col = reader_csr(n, texts)
+    np.testing.assert_array_equal(off, ref_off)
+    np.testing.assert_array_equal(col, ref_col)
+
+
+@pytest.mark.parametrize("chunk", [None, "64"])
+@pytest.mark.parametrize("text,status", [
+    ("0 1\n1 x\n", G.GRE_IO_ERROR),
+    ("0 1\n1 9\n", G.GRE_INVALID_ARG),          # vertex 9 >= n = 4
+    ("0 1\n1 2 3\n", G.GRE_IO_ERROR),           # a third token
+    ("0 1\n  \n", G.GRE_IO_ERROR),              # spaces only
+    ("0 1\n 2\n", G.GRE_IO_ERROR),
+    ("0 99999999999\n1 x\n", G.GRE_INVALID_ARG),  # the first bad line decides
+    ("1 x\n0 99999999999\n", G.GRE_IO_ERROR),
+])
+def test_bad_lines_rejected_with_loader_codes(monkeypatch, chunk, text, status):
+    if chunk:
+        monkeypatch.setenv("GRE_INGEST_CHUNK", chunk)
+    with tempfile.TemporaryDirectory() as td:
+        p = write(td, 4, ["0 1\n" * 50 + text])
+        with pytest.raises(G.GreError) as e:
+            G.Graph.ingress(p)
+        assert e.value.status == status
+
+
+def test_line_longer_than_a_chunk_is_an_io_error(monkeypatch):
+    monkeypatch.setenv("GRE_INGEST_CHUNK", "64")
+    with tempfile.TemporaryDirectory() as td:
+        p = write(td, 4, ["0 1\n" + "0" * 100 + "1 2\n"])
+        with pytest.raises(G.GreError) as e:
+            G.Graph.ingress(p)
+        assert e.value.status == G.GRE_IO_ERROR
+
+
+def test_empty_and_comment_only_files():
+    with tempfile.TemporaryDirectory() as td:
+        g = G.Graph.ingress(write(td, 3, ["", "# nothing\n\n", "2 0"]), G.InOut)
+    off, col = g.csr()
+    np.testing.assert_array_equal(off, [0, 0, 0, 1])
+    np.testing.assert_array_equal(col, [0])
+
+
+def test_rmat_text_round_trip_relabelled():
+    n, off, col = G.rmat_host(14, 16, 21, True)
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "r")
+        G.write_edgelists(p, n, off, col, 4)
+        g = G.Graph.ingress(p, G.InOut, symmetric=True, reorder=True)
+    o2, c2 = g.csr()
+    np.testing.assert_array_equal(o2, off)
+    np.testing.assert_array_equal(c2, col)
