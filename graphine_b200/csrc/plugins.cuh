@@ -107,6 +107,108 @@ struct VcSSSP {
   void reduce() {}
 };
 
+// PageRank_delta (Kernels/PageRank.hpp:129-197): only the change of a vertex's rank travels; a
+// vertex stays active while its change exceeds err.
+struct VcPageRankDelta {
+  typedef double msg_t;
+  double* pr;
+  double* scat;
+  double* comb;
+  const uint32_t* outdeg;
+  double tele;  // dampingFactor = 0.15 (PageRank.hpp:131)
+  double d;     // 1 - 0.15
+  double err;   // 1e-5 (PageRank.hpp:132)
+  __device__ bool init(uint32_t v) {
+    pr[v] = tele;
+    const uint32_t od = outdeg[v];
+    if (od > 0) {
+      scat[v] = pr[v] / (double)od;
+      return true;
+    }
+    return false;
+  }
+  template <class Ctx>
+  __device__ void scatter(Ctx& ctx, uint32_t u, uint32_t v, uint64_t) { ctx.sendMessage(v, scat[u]); }
+  __device__ bool combine(uint32_t v, const double& m) {
+    atomicAdd(comb + v, m);
+    return true;
+  }
+  __device__ bool apply(uint32_t v) {
+    const double delta = d * comb[v];
+    pr[v] += delta;
+    comb[v] = 0.0;
+    const uint32_t od = outdeg[v];
+    if (delta > err && od > 0) {
+      scat[v] = delta / (double)od;
+      return true;
+    }
+    return false;
+  }
+  __device__ bool assert_to_halt(uint32_t) { return true; }
+  void reduce() {}
+};
+
+// SSSP with predecessors (Kernels/SSSP1.hpp:62-95).  A state packs (dist << 32 | pred), pred a
+// caller vertex id, so one 64-bit atomicMin keeps the pair consistent.  combine reports an
+// improvement only when the distance drops (a tie with a smaller pred updates pred without
+// activating the vertex), so the active sets equal the reference's; among senders at equal
+// distance the reference keeps whichever message arrived first, this keeps the smallest id.
+struct VcSSSP1 {
+  typedef unsigned long long msg_t;
+  unsigned long long* states;
+  uint32_t* last;
+  const uint32_t* w;
+  const uint32_t* vid;  // get_vid: internal -> caller id, null = identity
+  __device__ bool init(uint32_t v) {
+    const unsigned long long me = vid ? vid[v] : v;
+    states[v] = me;  // dist 0, pred = self
+    last[v] = 0;
+    return true;
+  }
+  template <class Ctx>
+  __device__ void scatter(Ctx& ctx, uint32_t u, uint32_t v, uint64_t arc) {
+    const uint32_t dist = last[u] + w[arc];
+    ctx.sendMessage(v, ((unsigned long long)dist << 32) | (vid ? vid[u] : u));
+  }
+  __device__ bool combine(uint32_t v, const unsigned long long& m) {
+    if (!(m < states[v])) return false;
+    const unsigned long long old = atomicMin(states + v, m);
+    return (uint32_t)(m >> 32) < (uint32_t)(old >> 32);
+  }
+  __device__ bool apply(uint32_t v) {
+    last[v] = (uint32_t)(states[v] >> 32);
+    return true;
+  }
+  __device__ bool assert_to_halt(uint32_t) { return true; }
+  void reduce() {}
+};
+
+// CountIn (Kernels/CountIn.hpp:33-56): every vertex sends 1 along its arcs of the run's
+// direction; apply stores the count received.  One superstep in the reference driver.
+struct VcCountIn {
+  typedef int32_t msg_t;
+  int32_t* cn;
+  int32_t* scat;
+  int32_t* comb;
+  __device__ bool init(uint32_t v) {
+    cn[v] = 0;
+    scat[v] = 1;
+    return true;
+  }
+  template <class Ctx>
+  __device__ void scatter(Ctx& ctx, uint32_t u, uint32_t v, uint64_t) { ctx.sendMessage(v, scat[u]); }
+  __device__ bool combine(uint32_t v, const int32_t& m) {
+    atomicAdd(comb + v, m);
+    return true;
+  }
+  __device__ bool apply(uint32_t v) {
+    cn[v] = comb[v];
+    return false;
+  }
+  __device__ bool assert_to_halt(uint32_t) { return true; }
+  void reduce() {}
+};
+
 // ConnectedComponents (Kernels/CC.hpp:33-67): min-vid label propagation.  Labels are vids,
 // stored as uint32 (every vid fits).
 struct VcCC {

@@ -154,6 +154,102 @@ int gre_vc_sssp(gre_graph g, uint32_t src, uint32_t max_supersteps, uint32_t* di
   return last_active ? GRE_UNFINISHED : GRE_SUCCESS;
 }
 
+int gre_vc_pagerank_delta(gre_graph g, uint32_t max_supersteps, double* pr, gre_stats* st) {
+  if (!g || !pr) return GRE_NULL;
+  GRE_CHECK(use_graph(g));
+  stats_reset(st);
+  const uint64_t n = g->n;
+  double *dpr, *scat, *comb;
+  void* scratch;
+  GRE_CHECK(ws_array(g, WS_A, n, &dpr));
+  GRE_CHECK(ws_array(g, WS_B, n, &scat));
+  GRE_CHECK(ws_array(g, WS_C, n, &comb));
+  GRE_CHECK(g->ws.get(WS_D, vc_scratch_bytes(n), &scratch));
+  RunTimer timer(g);
+  GRE_CUDA(cudaMemsetAsync(comb, 0, sizeof(double) * n, g->stream));  // allocCombineData(pr_combine, 0.0)
+  VcPageRankDelta vc{dpr, scat, comb, g->outdeg, 0.15, 1.0 - 0.15, 1e-5};
+  SourceSet all;
+  all.all = true;
+  uint64_t last_active = 0;
+  GRE_CHECK(run_engine(g, vc, GRE_DIR_OUT, all, max_supersteps, scratch, st, nullptr, &last_active));
+  GRE_CHECK(emit(g, pr, dpr, WS_OUTBUF));
+  GRE_CHECK(timer.stop(st));
+  if (st) st->traversed_edges = st->arcs_traversed;
+  return last_active ? GRE_UNFINISHED : GRE_SUCCESS;
+}
+
+__global__ void k_split_sssp1(uint64_t n, const unsigned long long* __restrict__ states, uint32_t* __restrict__ dist,
+                              unsigned long long* __restrict__ pred) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x) {
+    const unsigned long long x = states[v];
+    const uint32_t d = (uint32_t)(x >> 32);
+    dist[v] = d;
+    pred[v] = d == 0xffffffffu ? ~0ull : (x & 0xffffffffull);  // _Data(): pred -1 when unreached
+  }
+}
+
+int gre_vc_sssp1(gre_graph g, uint32_t src, uint32_t max_supersteps, uint32_t* dist, uint64_t* pred, gre_stats* st) {
+  if (!g || !dist || !pred) return GRE_NULL;
+  if (!g->w32) {
+    set_error("gre_vc_sssp1: the graph has no uint32 weights (gre_graph_set_weights_*)");
+    return GRE_INVALID_ARG;
+  }
+  GRE_CHECK(use_graph(g));
+  std::vector<uint32_t> hs(1, src);
+  GRE_CHECK(map_ids(g, &hs, "gre_vc_sssp1"));
+  stats_reset(st);
+  const uint64_t n = g->n;
+  unsigned long long *states, *dpred;
+  uint32_t *last, *ddist;
+  const uint32_t* dsrc;
+  void* scratch;
+  GRE_CHECK(ws_array(g, WS_A, n, &states));
+  GRE_CHECK(ws_array(g, WS_B, n, &last));
+  GRE_CHECK(ws_array(g, WS_C, n, &ddist));
+  GRE_CHECK(ws_array(g, WS_F, n, &dpred));
+  GRE_CHECK(g->ws.get(WS_D, vc_scratch_bytes(n), &scratch));
+  RunTimer timer(g);
+  GRE_CHECK(stage_input(g, hs.data(), 1, WS_E, &dsrc));
+  GRE_CUDA(cudaMemsetAsync(states, 0xff, sizeof(unsigned long long) * n, g->stream));  // _Data(): dist max, pred -1
+  GRE_CUDA(cudaMemsetAsync(last, 0xff, sizeof(uint32_t) * n, g->stream));
+  VcSSSP1 vc{states, last, g->w32, g->perm};
+  SourceSet s;
+  s.dev_vertices = dsrc;
+  s.count = 1;
+  uint64_t last_active = 0;
+  GRE_CHECK(run_engine(g, vc, GRE_DIR_OUT, s, max_supersteps, scratch, st, nullptr, &last_active));
+  k_split_sssp1<<<grid_for(n, 256), 256, 0, g->stream>>>(n, states, ddist, dpred);
+  GRE_LAUNCH_CHECK();
+  GRE_CHECK(emit(g, dist, ddist, WS_OUTBUF));
+  GRE_CHECK(emit(g, (unsigned long long*)pred, dpred, WS_OUTBUF2));
+  GRE_CHECK(timer.stop(st));
+  return last_active ? GRE_UNFINISHED : GRE_SUCCESS;
+}
+
+int gre_vc_count_in(gre_graph g, int dir, uint32_t max_supersteps, int32_t* count, gre_stats* st) {
+  if (!g || !count) return GRE_NULL;
+  if (dir < GRE_DIR_OUT || dir > GRE_DIR_INOUT) return GRE_INVALID_ARG;
+  GRE_CHECK(use_graph(g));
+  stats_reset(st);
+  const uint64_t n = g->n;
+  int32_t *cn, *scat, *comb;
+  void* scratch;
+  GRE_CHECK(ws_array(g, WS_A, n, &cn));
+  GRE_CHECK(ws_array(g, WS_B, n, &scat));
+  GRE_CHECK(ws_array(g, WS_C, n, &comb));
+  GRE_CHECK(g->ws.get(WS_D, vc_scratch_bytes(n), &scratch));
+  RunTimer timer(g);
+  GRE_CUDA(cudaMemsetAsync(cn, 0, sizeof(int32_t) * n, g->stream));
+  GRE_CUDA(cudaMemsetAsync(comb, 0, sizeof(int32_t) * n, g->stream));  // allocCombineData(cn_combine, 0)
+  VcCountIn vc{cn, scat, comb};
+  SourceSet all;
+  all.all = true;
+  GRE_CHECK(run_engine(g, vc, dir, all, max_supersteps, scratch, st, nullptr, nullptr));
+  GRE_CHECK(emit(g, count, cn, WS_OUTBUF));
+  GRE_CHECK(timer.stop(st));
+  return GRE_SUCCESS;
+}
+
 int gre_vc_cc(gre_graph g, uint32_t* label, gre_stats* st) {
   if (!g || !label) return GRE_NULL;
   GRE_CHECK(use_graph(g));

@@ -120,6 +120,9 @@ def lib() -> C.CDLL:
             "gre_vc_bfs": (I32, [P, U32, I32, P, P, S]),
             "gre_vc_sssp": (I32, [P, U32, U32, P, S]),
             "gre_vc_cc": (I32, [P, P, S]),
+            "gre_vc_pagerank_delta": (I32, [P, U32, P, S]),
+            "gre_vc_sssp1": (I32, [P, U32, U32, P, P, S]),
+            "gre_vc_count_in": (I32, [P, I32, U32, P, S]),
             "gre_vc_bc": (I32, [P, P, U32, P, S]),
             "gre_pagerank": (I32, [P, I32, D, U32, P, S]),
             "gre_bfs": (I32, [P, P, U32, P, S]),
@@ -352,6 +355,34 @@ def vc_sssp(g: Graph, src: int, max_supersteps: int = 1024, out=None):
     st = _stats()
     status = _check(lib().gre_vc_sssp(g._h, int(src), max_supersteps, _ptr(out), C.byref(st)), "gre_vc_sssp")
     return out, Stats._from(st), status
+
+
+def vc_pagerank_delta(g: Graph, max_supersteps: int = 1024, out=None):
+    """PageRank_delta on the device engine; returns (pr, stats, status) (GRE_UNFINISHED if capped)."""
+    out = _out(out, g.n, np.float64)
+    st = _stats()
+    status = lib().gre_vc_pagerank_delta(g._h, max_supersteps, _ptr(out), C.byref(st))
+    if status not in (GRE_SUCCESS, GRE_UNFINISHED):
+        _check(status, "gre_vc_pagerank_delta")
+    return out, Stats._from(st), status
+
+
+def vc_sssp1(g: Graph, src: int, max_supersteps: int = 1024):
+    """SSSP1 (distances + predecessors); returns (dist, pred, stats, status)."""
+    dist = np.empty(g.n, np.uint32)
+    pred = np.empty(g.n, np.uint64)
+    st = _stats()
+    status = lib().gre_vc_sssp1(g._h, src, max_supersteps, _ptr(dist), _ptr(pred), C.byref(st))
+    if status not in (GRE_SUCCESS, GRE_UNFINISHED):
+        _check(status, "gre_vc_sssp1")
+    return dist, pred, Stats._from(st), status
+
+
+def vc_count_in(g: Graph, dir: int = In, max_supersteps: int = 1, out=None):
+    out = _out(out, g.n, np.int32)
+    st = _stats()
+    _check(lib().gre_vc_count_in(g._h, dir, max_supersteps, _ptr(out), C.byref(st)), "gre_vc_count_in")
+    return out, Stats._from(st)
 
 
 def vc_cc(g: Graph, out=None):

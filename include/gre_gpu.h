@@ -167,6 +167,19 @@ int gre_vc_sssp(gre_graph g, uint32_t src, uint32_t max_supersteps, uint32_t* di
 /* usr/test_cc.cpp: ConnectedComponents (Kernels/CC.hpp), run<InOut>, setALL.  label: n
  * uint32 = minimum vid of the component. */
 int gre_vc_cc(gre_graph g, uint32_t* label, gre_stats* st);
+/* Kernels/PageRank.hpp:129-197 (PageRank_delta): only rank changes propagate; a vertex stays
+ * active while its change exceeds 1e-5.  run<Out> from every vertex; GRE_UNFINISHED when
+ * max_supersteps ran out first. */
+int gre_vc_pagerank_delta(gre_graph g, uint32_t max_supersteps, double* pr, gre_stats* st);
+/* Kernels/SSSP1.hpp:62-95: SSSP with predecessors (pred = the caller id of the vertex whose
+ * message set the distance; the source is its own pred, unreached vertices UINT64_MAX with
+ * UINT32_MAX distance).  Distances equal the reference's; among predecessors at equal distance
+ * the smallest id is kept (the reference keeps whichever message arrived first). */
+int gre_vc_sssp1(gre_graph g, uint32_t src, uint32_t max_supersteps, uint32_t* dist, uint64_t* pred,
+                 gre_stats* st);
+/* Kernels/CountIn.hpp:33-56 with usr/test_cIn.cpp's driver (every vertex active, the reference
+ * runs run<In> for one superstep): count[v] = messages v received along `dir`. */
+int gre_vc_count_in(gre_graph g, int dir, uint32_t max_supersteps, int32_t* count, gre_stats* st);
 /* usr/test_bc.cpp looped over sources: Forward run<Out> + Backward run<In> per level
  * (Kernels/BC.hpp); bc[v] = sum over sources s != v of dep_s(v).  bc: n doubles. */
 int gre_vc_bc(gre_graph g, const uint32_t* srcs, uint32_t nsrc, double* bc, gre_stats* st);

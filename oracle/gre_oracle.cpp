@@ -256,6 +256,93 @@ struct SSSPVC : PluginBase {
   }
 };
 
+// PageRank_delta (Kernels/PageRank.hpp:129-197): init pr = 0.15, scatter pr/outdeg; combine
+// sums; apply adds delta = 0.85 * sum and stays active while delta > 1e-5 (and outdeg > 0),
+// scattering delta/outdeg.
+struct PageRankDeltaVC : PluginBase {
+  typedef double msg_t;
+  const OGraph* g;
+  std::vector<double> pr, scat, comb;
+  bool init(uint32_t v) {
+    pr[v] = 0.15;
+    if (g->outdeg[v] > 0) {
+      scat[v] = pr[v] / (double)g->outdeg[v];
+      return true;
+    }
+    return false;
+  }
+  template <class C>
+  void scatter(C& ctx, uint32_t u, uint32_t v, uint64_t) { ctx.sendMessage(v, scat[u]); }
+  bool combine(uint32_t v, double m) {
+    comb[v] += m;
+    return true;
+  }
+  bool apply(uint32_t v) {
+    const double delta = (1.0 - 0.15) * comb[v];
+    pr[v] += delta;
+    comb[v] = 0.0;
+    if (delta > 1e-5 && g->outdeg[v] > 0) {
+      scat[v] = delta / (double)g->outdeg[v];
+      return true;
+    }
+    return false;
+  }
+};
+
+// SSSP with predecessors (Kernels/SSSP1.hpp:62-95): a message carries (sender, distance); a
+// strictly shorter distance replaces both fields.
+struct SSSP1VC : PluginBase {
+  typedef std::pair<uint32_t, uint32_t> msg_t;  // (pred, dist)
+  std::vector<uint32_t> dist, last;
+  std::vector<uint64_t> pred;
+  uint64_t wseed;
+  const uint32_t* warc;
+  bool init(uint32_t v) {
+    pred[v] = v;
+    dist[v] = 0;
+    last[v] = 0;
+    return true;
+  }
+  template <class C>
+  void scatter(C& ctx, uint32_t u, uint32_t v, uint64_t arc) {
+    const uint32_t w = warc ? warc[arc] : gre_oracle::sssp_weight(wseed, u, v);
+    ctx.sendMessage(v, msg_t(u, last[u] + w));
+  }
+  bool combine(uint32_t v, const msg_t& m) {
+    if (m.second < dist[v]) {
+      dist[v] = m.second;
+      pred[v] = m.first;
+      return true;
+    }
+    return false;
+  }
+  bool apply(uint32_t v) {
+    last[v] = dist[v];
+    return true;
+  }
+};
+
+// CountIn (Kernels/CountIn.hpp:33-56): every vertex sends 1; apply stores the count received.
+struct CountInVC : PluginBase {
+  typedef int32_t msg_t;
+  std::vector<int32_t> cn, scat, comb;
+  bool init(uint32_t v) {
+    cn[v] = 0;
+    scat[v] = 1;
+    return true;
+  }
+  template <class C>
+  void scatter(C& ctx, uint32_t u, uint32_t v, uint64_t) { ctx.sendMessage(v, scat[u]); }
+  bool combine(uint32_t v, int32_t m) {
+    comb[v] += m;
+    return true;
+  }
+  bool apply(uint32_t v) {
+    cn[v] = comb[v];
+    return false;
+  }
+};
+
 // ConnectedComponents (Kernels/CC.hpp:33-67): min global vid label propagation.
 struct CCVC : PluginBase {
   typedef uint64_t msg_t;
@@ -535,6 +622,53 @@ int oracle_sssp_many(const oracle_graph* g, const uint32_t* srcs, uint32_t k, ui
 #pragma omp parallel for schedule(dynamic, 1)
   for (int64_t i = 0; i < (int64_t)k; ++i)
     oracle_sssp(g, srcs[i], wseed, warc, dist + (uint64_t)i * g->n, nullptr, 0, nullptr);
+  return 0;
+}
+
+// PageRank_delta, run<Out> from every vertex (usr/test_pagerank.cpp:65-74 with the
+// PageRank_delta typedef of line 22).
+int oracle_pagerank_delta(const oracle_graph* g, uint32_t max_ss, double* pr, uint64_t* counts, uint32_t cap, uint32_t* nss) {
+  PageRankDeltaVC vc;
+  vc.g = g;
+  vc.pr.assign(g->n, 0.0);
+  vc.scat.assign(g->n, 0.0);
+  vc.comb.assign(g->n, 0.0);
+  Trace tr;
+  run(*g, vc, DIR_OUT, nullptr, 0, max_ss, &tr);
+  memcpy(pr, vc.pr.data(), sizeof(double) * g->n);
+  copy_trace(tr, counts, cap, nss);
+  return 0;
+}
+
+// SSSP1 from one source, run<Out> (usr/test_sssp.cpp:58-69 with the SSSP1 include).
+int oracle_sssp1(const oracle_graph* g, uint32_t src, uint64_t wseed, const uint32_t* warc, uint32_t* dist, uint64_t* pred,
+                 uint64_t* counts, uint32_t cap, uint32_t* nss) {
+  SSSP1VC vc;
+  vc.dist.assign(g->n, 0xffffffffu);  // _Data(): dist max, pred -1
+  vc.pred.assign(g->n, ~0ull);
+  vc.last.assign(g->n, 0xffffffffu);
+  vc.wseed = wseed;
+  vc.warc = warc;
+  Trace tr;
+  run(*g, vc, DIR_OUT, &src, 1, 1024, &tr);
+  memcpy(dist, vc.dist.data(), sizeof(uint32_t) * g->n);
+  memcpy(pred, vc.pred.data(), sizeof(uint64_t) * g->n);
+  copy_trace(tr, counts, cap, nss);
+  return 0;
+}
+
+// CountIn with every vertex active along `dir` for max_ss supersteps (usr/test_cIn.cpp:30-40:
+// run<In>, one superstep).
+int oracle_count_in(const oracle_graph* g, int dir, uint32_t max_ss, int32_t* cn, uint64_t* counts, uint32_t cap,
+                    uint32_t* nss) {
+  CountInVC vc;
+  vc.cn.assign(g->n, 0);
+  vc.scat.assign(g->n, 0);
+  vc.comb.assign(g->n, 0);
+  Trace tr;
+  run(*g, vc, dir, nullptr, 0, max_ss, &tr);
+  memcpy(cn, vc.cn.data(), sizeof(int32_t) * g->n);
+  copy_trace(tr, counts, cap, nss);
   return 0;
 }
 

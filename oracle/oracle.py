@@ -56,6 +56,9 @@ def lib() -> C.CDLL:
             "oracle_pagerank_weighted": (I32, [P, P, P, D, U32, P]),
             "oracle_pagerank_adjoint": (I32, [P, P, P, P, D, U32, P, P, P]),
             "oracle_sssp_weight": (U32, [U64, U32, U32]),
+            "oracle_pagerank_delta": (I32, [P, U32, P, P, U32, C.POINTER(U32)]),
+            "oracle_sssp1": (I32, [P, U32, U64, P, P, P, P, U32, C.POINTER(U32)]),
+            "oracle_count_in": (I32, [P, I32, U32, P, P, U32, C.POINTER(U32)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -160,6 +163,29 @@ class Restatement:
         lib().oracle_sssp_many(self._h, _p(s), len(s), wseed, _p(w), _p(out))
         return out.reshape(len(s), self.n)
 
+    def pagerank_delta(self, max_supersteps: int = 1024):
+        pr = np.empty(self.n, dtype=np.float64)
+        counts = np.zeros(1024, dtype=np.uint64)
+        nss = C.c_uint32()
+        lib().oracle_pagerank_delta(self._h, max_supersteps, _p(pr), _p(counts), 1024, C.byref(nss))
+        return pr, self._trace(counts, nss)
+
+    def sssp1(self, src: int, wseed: int = 0, warc=None):
+        dist = np.empty(self.n, dtype=np.uint32)
+        pred = np.empty(self.n, dtype=np.uint64)
+        counts = np.zeros(1024, dtype=np.uint64)
+        nss = C.c_uint32()
+        w = None if warc is None else np.ascontiguousarray(warc, dtype=np.uint32)
+        lib().oracle_sssp1(self._h, int(src), wseed, _p(w), _p(dist), _p(pred), _p(counts), 1024, C.byref(nss))
+        return dist, pred, self._trace(counts, nss)
+
+    def count_in(self, dir: int = 1, max_supersteps: int = 1):
+        cn = np.empty(self.n, dtype=np.int32)
+        counts = np.zeros(1024, dtype=np.uint64)
+        nss = C.c_uint32()
+        lib().oracle_count_in(self._h, dir, max_supersteps, _p(cn), _p(counts), 1024, C.byref(nss))
+        return cn, self._trace(counts, nss)
+
     def cc(self):
         label = np.empty(self.n, dtype=np.uint64)
         counts = np.zeros(1024, dtype=np.uint64)
@@ -237,7 +263,8 @@ def _parse(stdout: str) -> RefRun:
 def run_reference(algo: str, prefix: str, *args, timeout: float = 600.0):
     """Run oracle/_ref/ref_<algo> on <prefix>; returns (array, RefRun)."""
     exe = os.path.join(REF_DIR, f"ref_{algo}")
-    dtype = {"pagerank": np.float64, "bfs": np.int32, "sssp": np.uint32, "cc": np.uint64, "bc": np.float64}[algo]
+    dtype = {"pagerank": np.float64, "bfs": np.int32, "sssp": np.uint32, "cc": np.uint64, "bc": np.float64,
+             "sssp1": np.uint8, "countin": np.int32}[algo]
     with tempfile.TemporaryDirectory() as td:
         out = os.path.join(td, "out.bin")
         p = subprocess.run([exe, prefix, out, *[str(a) for a in args]], capture_output=True, text=True, timeout=timeout)

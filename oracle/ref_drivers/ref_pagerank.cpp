@@ -2,7 +2,7 @@
 // PageRankIter / personalised plugins written against the reference's VertexCode API) on the
 // reference engine, np = 1.
 //
-//   ref_pagerank <prefix> <out.f64> gre|iter <supersteps> [repeats]
+//   ref_pagerank <prefix> <out.f64> gre|iter|delta <supersteps> [repeats]
 //   ref_pagerank <prefix> <out.f64> ppr <supersteps> <seed vertex> [<seed vertex> ...]
 // Writes n doubles per run (appended in seed order for ppr).  Mirrors usr/test_pagerank.cpp:
 // ingress<Out>, srcSet.setALL(), configMaxSupersteps, engine.run (= run<Out>).
@@ -107,6 +107,16 @@ int main(int argc, char** argv) {
       write_array(out, pr.pr, sizeof(double) * n);
       engine.finalize();
     }
+  } else if (variant == "delta") {  // the PageRank_delta typedef of usr/test_pagerank.cpp:22
+    PageRank_delta pr(g);
+    GRE::SynchronousEngine<PageRank_delta> engine(g, comm, pool, pr);
+    engine.initialize();
+    engine.configMaxSupersteps(supersteps);
+    comm.startTimer();
+    engine.run(srcSet, GRE::Par_ThreadPool);
+    report_run("pagerank_delta", comm.stopTimer(), engine.getSuperstepCount());
+    write_array(out, pr.pr, sizeof(double) * n);
+    engine.finalize();
   } else if (variant == "ppr") {
     write_array(out, "", 0);
     for (int a = 5; a < argc; ++a) {

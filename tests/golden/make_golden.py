@@ -58,6 +58,8 @@ def write_case(name: str, n: int, off: np.ndarray, col: np.ndarray, roots: np.nd
         res["pr_iter20"], res["pr_iter20_active"] = pr, np.array(run.active[0])
         pp, _ = O.run_reference("pagerank", prefix, "ppr", PR_SUPERSTEPS, *[int(r) for r in roots[:2]])
         res["ppr20"] = pp.reshape(-1, n)
+        pr, run = O.run_reference("pagerank", prefix, "delta", 1024)
+        res["prdelta"], res["prdelta_active"] = pr, np.array(run.active[0])
         if symmetric:
             lv, run = O.run_reference("bfs", prefix)
             assert "GRE_BFS_REACH_MISMATCH" not in run.stdout
@@ -65,6 +67,13 @@ def write_case(name: str, n: int, off: np.ndarray, col: np.ndarray, roots: np.nd
             res["bfs_active"] = _pad(run.active[0::2])  # runs alternate: BFS plugin, Forward levels
             dist, run = O.run_reference("sssp", prefix, WSEED)
             res["sssp_dist"], res["sssp_active"] = dist.reshape(-1, n), _pad(run.active)
+            raw, run = O.run_reference("sssp1", prefix, WSEED)
+            per = 12 * n  # n uint32 distances then n uint64 predecessors per root
+            res["sssp1_dist"] = np.stack([raw[i * per:i * per + 4 * n].view(np.uint32) for i in range(len(roots))])
+            res["sssp1_pred"] = np.stack([raw[i * per + 4 * n:(i + 1) * per].view(np.uint64) for i in range(len(roots))])
+            res["sssp1_active"] = _pad(run.active)
+            cnt, run = O.run_reference("countin", prefix)
+            res["countin"], res["countin_active"] = cnt, np.array(run.active[0])
             lab, run = O.run_reference("cc", prefix)
             res["cc_label"], res["cc_active"] = lab, np.array(run.active[0])
             b, run = O.run_reference("bc", prefix)

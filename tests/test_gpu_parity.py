@@ -123,6 +123,44 @@ def test_bc_golden(golden, name, reorder):
 
 
 @pytest.mark.parametrize("name", CASES)
+@REORDER
+def test_pagerank_delta_golden(golden, name, reorder):
+    case = golden[name]
+    g = graph_of(case, reorder)
+    pr, st, status = G.vc_pagerank_delta(g)
+    assert status == G.GRE_SUCCESS
+    assert rel_l1(pr, case["prdelta"]) <= TOL
+    assert st.active == list(case["prdelta_active"])
+
+
+@pytest.mark.parametrize("name", SYM)
+@REORDER
+def test_sssp1_golden(golden, name, reorder):
+    from test_oracle_golden import pred_tree_ok
+
+    case = golden[name]
+    g = graph_of(case, reorder)
+    wseed = int(case["wseed"])
+    g.set_weights_hash(wseed)
+    for i, r in enumerate(case["roots"]):
+        dist, pred, st, status = G.vc_sssp1(g, int(r))
+        assert status == G.GRE_SUCCESS
+        np.testing.assert_array_equal(dist, case["sssp1_dist"][i])
+        assert st.active == [x for x in case["sssp1_active"][i] if x >= 0]
+        assert pred_tree_ok(case["off"], case["col"], wseed, int(r), dist, pred)
+
+
+@pytest.mark.parametrize("name", SYM)
+@REORDER
+def test_count_in_golden(golden, name, reorder):
+    case = golden[name]
+    g = graph_of(case, reorder)
+    cn, st = G.vc_count_in(g, G.In, 1)
+    np.testing.assert_array_equal(cn, case["countin"])
+    assert st.active == list(case["countin_active"])
+
+
+@pytest.mark.parametrize("name", CASES)
 def test_loader_matches_fixture(golden, name):
     """gre_graph_load on the text files gives the fixture's CSR (file order within a source)."""
     case = golden[name]
