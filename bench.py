@@ -294,6 +294,7 @@ def run_ours(args, rank, world, local_rank):
         return [calls[k]() for k in names]
 
     dev_outs = (pr_d, lv_d, ds_d, cc_d)
+    sched = dict(zip(("lane_arcs", "cta_min", "hub_chunk"), g.row_schedule(True)))  # tuned on first use
     for i in range(args.warmup):
         suite(i, dev_outs)
     torch.cuda.synchronize()
@@ -382,7 +383,7 @@ def run_ours(args, rank, world, local_rank):
         "config": {"workload": f"GRE plain suite on RMAT scale {args.scale} EF16 symmetric: PageRank-{PR_ITERS} (power "
                                f"iteration, FP64), DO-BFS 1 src, SSSP 1 src (u32 w in [1,255]), CC",
                    "graph_n": n, "graph_arcs": m, "parallelism": f"replica x{world}",
-                   "row_schedule": dict(zip(("lane_arcs", "cta_min", "hub_chunk"), g.row_schedule(True))),
+                   "row_schedule": sched,
                    "l2": "inputs larger than L2 (graph > 126 MB)"},
         "per_algorithm": per_alg,
         "roofline": {"bound": "hbm", "kernel": "PageRank pull superstep (degree-binned row kernels)",

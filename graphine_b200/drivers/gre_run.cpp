@@ -1,7 +1,8 @@
 // gre_run — drop-in for the reference example drivers (usr/test_pagerank.cpp, test_bfs.cpp,
-// test_sssp.cpp, test_cc.cpp, test_bc.cpp) on libgre_gpu.so, written against gre/gre.hpp.
+// test_sssp.cpp, test_cc.cpp, test_cIn.cpp, test_bc.cpp) on libgre_gpu.so, written against
+// gre/gre.hpp.
 //
-//   gre_run <pagerank|pagerank_iter|bfs|sssp|cc|bc> <prefix> [ascii] [edgelists]
+//   gre_run <pagerank|pagerank_iter|pagerank_delta|bfs|sssp|sssp1|cc|cin|bc> <prefix> [ascii] [edgelists]
 //
 // Same inputs (<prefix>.meta, <prefix>.edges.<i>, <prefix>.roots, source = the first root as
 // the reference's src[1]) and the same per-superstep lines the reference engine prints
@@ -25,18 +26,19 @@ static void print_supersteps(const gre_stats& st) {
 
 int main(int argc, char** argv) {
   if (argc < 3) {
-    fprintf(stderr, "usage: %s pagerank|pagerank_iter|bfs|sssp|cc|bc prefix [ascii] [edgelists]\n", argv[0]);
+    fprintf(stderr, "usage: %s pagerank|pagerank_iter|pagerank_delta|bfs|sssp|sssp1|cc|cin|bc prefix [ascii] [edgelists]\n",
+            argv[0]);
     return 2;
   }
   const std::string algo(argv[1]), prefix(argv[2]);
   try {
     gre::DistributedGraph g;
-    const bool in_out = algo == "bfs" || algo == "cc" || algo == "bc";
+    const bool in_out = algo == "bfs" || algo == "cc" || algo == "bc" || algo == "cin";
     if (in_out) g.ingress<gre::InOut>(prefix);
     else g.ingress<gre::Out>(prefix);
     std::vector<uint32_t> roots(1024);
     uint32_t nroots = 0;
-    if (algo == "bfs" || algo == "sssp" || algo == "bc") {
+    if (algo == "bfs" || algo == "sssp" || algo == "sssp1" || algo == "bc") {
       int s = gre_read_roots(prefix.c_str(), roots.data(), (uint32_t)roots.size(), &nroots);
       if ((s != GRE_SUCCESS && s != GRE_NOBUFFER) || nroots == 0) {
         fprintf(stderr, "Err in reading src vertex from file.\n");
@@ -58,6 +60,37 @@ int main(int argc, char** argv) {
       for (double x : pr.pr) sum += x;
       print_supersteps(st);
       printf("Sum of pr: %.15g\n", sum);
+    } else if (algo == "pagerank_delta") {  // usr/test_pagerank.cpp:22 with the PageRank_delta typedef
+      src.setALL();
+      gre::PageRank_delta pr(g);
+      gre::SynchronousEngine<gre::PageRank_delta> engine(g, pr);
+      engine.run<gre::Out>(src);
+      st = engine.stats();
+      double sum = 0;
+      for (double x : pr.pr) sum += x;
+      print_supersteps(st);
+      printf("Sum of pr: %.15g\n", sum);
+    } else if (algo == "sssp1") {
+      const char* ws = getenv("GRE_WSEED");
+      g.loadEdgePropertyHash(ws ? strtoull(ws, nullptr, 10) : 1);
+      src.addVertex(roots[0], g);
+      gre::SSSP1 sssp(g);
+      gre::SynchronousEngine<gre::SSSP1> engine(g, sssp);
+      engine.configMaxSupersteps(128);
+      engine.run<gre::Out>(src);
+      st = engine.stats();
+      print_supersteps(st);
+    } else if (algo == "cin") {  // usr/test_cIn.cpp
+      src.setALL();
+      gre::CountIn cin(g);
+      gre::SynchronousEngine<gre::CountIn> engine(g, cin);
+      engine.configMaxSupersteps(1);
+      engine.run<gre::In>(src);
+      st = engine.stats();
+      print_supersteps(st);
+      long total = 0;
+      for (int32_t c : cin.cn) total += c;
+      printf("Number of in edges: %ld\n", total);
     } else if (algo == "bfs") {
       src.addVertex(roots[0], g);
       gre::BFS bfs(g);

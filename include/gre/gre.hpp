@@ -111,6 +111,22 @@ struct ConnectedComponents {
   DistributedGraph& graph;
   std::vector<uint32_t> cc;  // minimum vid of the component
 };
+struct PageRank_delta {  // Kernels/PageRank.hpp:129-197
+  explicit PageRank_delta(DistributedGraph& g) : graph(g) {}
+  DistributedGraph& graph;
+  std::vector<double> pr;
+};
+struct SSSP1 {  // Kernels/SSSP1.hpp: distances and predecessors
+  explicit SSSP1(DistributedGraph& g) : graph(g) {}
+  DistributedGraph& graph;
+  std::vector<uint32_t> dist;
+  std::vector<uint64_t> pred;  // caller vid of the predecessor; UINT64_MAX when unreached
+};
+struct CountIn {  // Kernels/CountIn.hpp
+  explicit CountIn(DistributedGraph& g) : graph(g) {}
+  DistributedGraph& graph;
+  std::vector<int32_t> cn;
+};
 struct BC {  // usr/test_bc.cpp's Forward + Backward, accumulated over the sources
   explicit BC(DistributedGraph& g) : graph(g) {}
   DistributedGraph& graph;
@@ -149,6 +165,19 @@ class SynchronousEngine {
   void runImpl(Dir, const SourceVertexSet& s, SSSP& p) {
     p.states.resize(g_.get_num_masters());
     check(gre_vc_sssp(g_.handle(), *first(s), max_, p.states.data(), &st_), "gre_vc_sssp");
+  }
+  void runImpl(Dir, const SourceVertexSet&, PageRank_delta& p) {
+    p.pr.resize(g_.get_num_masters());
+    check(gre_vc_pagerank_delta(g_.handle(), max_, p.pr.data(), &st_), "gre_vc_pagerank_delta");
+  }
+  void runImpl(Dir, const SourceVertexSet& s, SSSP1& p) {
+    p.dist.resize(g_.get_num_masters());
+    p.pred.resize(g_.get_num_masters());
+    check(gre_vc_sssp1(g_.handle(), *first(s), max_, p.dist.data(), p.pred.data(), &st_), "gre_vc_sssp1");
+  }
+  void runImpl(Dir dir, const SourceVertexSet&, CountIn& c) {
+    c.cn.resize(g_.get_num_masters());
+    check(gre_vc_count_in(g_.handle(), (int)dir, max_, c.cn.data(), &st_), "gre_vc_count_in");
   }
   void runImpl(Dir, const SourceVertexSet&, ConnectedComponents& c) {
     c.cc.resize(g_.get_num_masters());
