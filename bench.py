@@ -360,10 +360,12 @@ def run_ours(args, rank, world, local_rank):
                       "share": v["ms"] / tot_ms}
     extra = {}
     if not args.no_batched:
-        # one 64-source betweenness batch on the scale-26 graph, then the batched-vs-looped block
-        srcs = np.sort(rng.choice(nz, size=BC_SOURCES, replace=False)).astype(np.uint32)
+        # sampled betweenness on the scale-26 graph in batches of 64 sources (one batch by
+        # default, --bc-sources 1024 for the full sample), then the batched-vs-looped block
+        srcs = np.sort(rng.choice(nz, size=args.bc_sources, replace=False)).astype(np.uint32)
         _, s = G.bc(g, srcs, batched=True)
-        extra["bc64_s26"] = {"ms": s.device_ms, "gteps": s.traversed_edges / (s.device_ms * 1e-3) / 1e9}
+        extra[f"bc{args.bc_sources}_s26"] = {"ms": s.device_ms, "gteps": s.traversed_edges / (s.device_ms * 1e-3) / 1e9,
+                                             "sources": args.bc_sources}
         del g
         torch.cuda.empty_cache()
         extra.update(batched_block(G, local_rank, args.batch_scale, 77))
@@ -408,6 +410,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=int, default=26)
     ap.add_argument("--batch-scale", type=int, default=20)
+    ap.add_argument("--bc-sources", type=int, default=BC_SOURCES, help="sampled BC sources at the main scale")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-reorder", action="store_true", help="keep the generated vertex order")
     ap.add_argument("--only", default="", help="comma-separated subset of the suite (profiling runs)")
