@@ -288,6 +288,7 @@ void destroy_graph(gre_graph g) {
   cudaFree(g->perm);
   cudaFree(g->iperm);
   cudaFree(g->arc_rank);
+  g->sssp_split.release();
   g->ws.release();
   if (g->ev0) cudaEventDestroy(g->ev0);
   if (g->ev1) cudaEventDestroy(g->ev1);
@@ -377,6 +378,7 @@ int finish_graph(gre_graph g) {
 
 // Drops everything derived from the CSR (degrees, CSC, arc maps, bins, chunk tables).
 static void drop_derived(gre_graph g) {
+  g->sssp_split.release();
   const bool alias = (g->roff == g->off);
   if (!alias) {
     cudaFree(g->roff);
@@ -845,6 +847,7 @@ int gre_graph_set_weights_u32(gre_graph g, const uint32_t* w) {
   if (!g->w32) GRE_CUDA(cudaMalloc(&g->w32, sizeof(uint32_t) * (g->m ? g->m : 1)));
   GRE_CHECK(upload_arcs(g, w, 4, g->w32));
   g->w32_mean = -1.0;
+  g->sssp_split.release();
   GRE_CUDA(cudaStreamSynchronize(g->stream));
   return GRE_SUCCESS;
 }
@@ -856,6 +859,7 @@ int gre_graph_set_weights_hash(gre_graph g, uint64_t wseed) {
   if (g->m) k_hash_weights<<<grid_for(g->m, 256), 256, 0, g->stream>>>(g->n, g->m, g->off, g->col, g->perm, wseed, g->w32);
   GRE_LAUNCH_CHECK();
   g->w32_mean = -1.0;
+  g->sssp_split.release();
   GRE_CUDA(cudaStreamSynchronize(g->stream));
   return GRE_SUCCESS;
 }

@@ -116,6 +116,21 @@ struct gre_graph_s {
   // weights
   uint32_t* w32 = nullptr;
   double w32_mean = -1.0;  // mean of w32, computed on first use (-1: unknown)
+  // SSSP light/heavy arc split for bucket width `delta` (sssp.cu): each row's arcs reordered so
+  // the light ones (w < delta) come first; heavy ones start at lsplit[v].  Built on first use,
+  // dropped when the weights or the arc order change.
+  struct SsspSplit {
+    uint32_t* col = nullptr;
+    uint32_t* w = nullptr;
+    uint64_t* lsplit = nullptr;
+    uint32_t delta = 0;
+    void release() {
+      cudaFree(col);
+      cudaFree(w);
+      cudaFree(lsplit);
+      *this = SsspSplit();
+    }
+  } sssp_split;
   double* w64 = nullptr;
   double* rw64 = nullptr;  // FP64 weights in CSC order (built on demand)
   uint64_t max_outdeg = 0, max_indeg = 0;
