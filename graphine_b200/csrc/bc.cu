@@ -333,9 +333,11 @@ struct BcM {
       for (int i = 0; i < cnt; ++i) {
         const uint64_t row = (uint64_t)su[i] * 64;
         const unsigned long long mm = sm[i];
-        if ((mm >> lane) & 1ull) acc0 = add(acc0, FWD ? sigma[row + lane] : dep_term(dep[row + lane], sigma[row + lane]));
-        if ((mm >> (lane + 32)) & 1ull)
-          acc1 = add(acc1, FWD ? sigma[row + lane + 32] : dep_term(dep[row + lane + 32], sigma[row + lane + 32]));
+        // forward: sigma holds path counts; backward: the children's entries already hold their
+        // pull weights dep_term(dep, sigma) (k_bcm_weights), the same value the looped path
+        // computes per arc
+        if ((mm >> lane) & 1ull) acc0 = add(acc0, sigma[row + lane]);
+        if ((mm >> (lane + 32)) & 1ull) acc1 = add(acc1, sigma[row + lane + 32]);
       }
       __syncwarp();
     }
@@ -355,6 +357,26 @@ struct BcM {
     }
   }
 };
+
+// Backward: once the dependencies of a level are final, each of its (vertex, source) entries of
+// sigma is replaced by the weight its parents pull, dep_term(dep, sigma) = (1 + dep) / sigma:
+// one division per entry instead of one per arc and source, and one load per term instead of
+// two.  The entry's sigma is not read again (its own dependency is already stored).
+__global__ void __launch_bounds__(256) k_bcm_weights(const uint32_t* __restrict__ list, const unsigned int* __restrict__ count,
+                                                     const unsigned long long* __restrict__ F, double* __restrict__ sigma,
+                                                     const double* __restrict__ dep) {
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t cnt = *count;
+  for (uint64_t i = warp; i < cnt; i += nwarps) {
+    const uint32_t w = list[i];
+    const unsigned long long word = F[w];
+    const uint64_t row = (uint64_t)w * 64;
+    if ((word >> lane) & 1ull) sigma[row + lane] = dep_term(dep[row + lane], sigma[row + lane]);
+    if ((word >> (lane + 32)) & 1ull) sigma[row + lane + 32] = dep_term(dep[row + lane + 32], sigma[row + lane + 32]);
+  }
+}
 
 template <bool FWD>
 __global__ void __launch_bounds__(256) k_bcm_rows(const uint32_t* __restrict__ list, const unsigned int* __restrict__ count, BcM B,
@@ -499,6 +521,9 @@ static int bc_batched(gre_graph g, const std::vector<uint32_t>& hs, double* dbc,
     unsigned long long* F = (unsigned long long*)g->bc_fpool;
     auto level_pass = [&](bool fwd, uint64_t d) -> int {
       BcM B{g->roff, g->rcol, fwd ? F + (d - 1) * n : F + (d + 1) * n, F + d * n, sigma, dep};
+      // backward: `list` still holds F_{d+1} (built by the previous pass: the last forward pass
+      // for the deepest level), whose dependencies are final
+      if (!fwd) k_bcm_weights<<<sms * 8, 256, 0, g->stream>>>(list, (unsigned int*)cnt, F + (d + 1) * n, sigma, dep);
       GRE_CUDA(cudaMemsetAsync(cnt, 0, 4, g->stream));
       k_bcm_list<<<grid_for(n, 256, 8), 256, 0, g->stream>>>(n, F + d * n, list, (unsigned int*)cnt);
       const int grid = sms * 8;
