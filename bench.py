@@ -294,7 +294,7 @@ def run_ours(args, rank, world, local_rank):
         return [calls[k]() for k in names]
 
     dev_outs = (pr_d, lv_d, ds_d, cc_d)
-    sched = dict(zip(("lane_arcs", "cta_min", "hub_chunk"), g.row_schedule(True)))  # tuned on first use
+    sched = dict(zip(("lane_arcs", "cta_min", "hub_chunk", "seg_window"), g.row_schedule(True)))  # tuned on first use
     for i in range(args.warmup):
         suite(i, dev_outs)
     torch.cuda.synchronize()

@@ -1,5 +1,9 @@
 // Degree bins of a CSR/CSC and the autotuner that chooses their threads-per-row schedule.
 //
+// The schedule also decides whether the rows above cta_min are split at source windows (rows
+// sorted by column only): their gathers then run window after window, so each window's share
+// of the gathered array stays in L2 instead of being fetched again from HBM for every hub.
+//
 // The reference gives every active vertex to one worker thread and walks its arcs serially
 // (Engine.hpp:592-625); on the GPU a row's arcs are spread over 1..32 lanes, a CTA, or several
 // CTAs depending on its degree (rows.cuh).  Which degrees go to which width is a schedule
@@ -13,7 +17,8 @@
 //
 // GRE_TUNE=0 in the environment turns the measurement off (the default schedule is used), and
 // graphs with fewer than 2^22 arcs always use the default: their supersteps are too short to
-// time apart from launch overhead.
+// time apart from launch overhead.  GRE_ROW_SCHEDULE=lane_arcs,cta_min,hub_chunk,seg_window
+// imposes a schedule (tests use it to reach every kernel on small graphs).
 #include <cub/cub.cuh>
 
 #include <cstdlib>
@@ -96,16 +101,114 @@ struct ProbeStore {
 
 int cub_temp(gre_graph g, size_t bytes, void** p) { return g->ws.get(WS_CUB, bytes, p); }
 
+}  // namespace
+
 void free_bins(DegreeBins& B) {
   cudaFree(B.rows);
   cudaFree(B.hub_chunk_row);
   cudaFree(B.hub_chunk_begin);
   cudaFree(B.hub_chunk_first);
+  cudaFree(B.seg_rows);
+  cudaFree(B.seg_first);
+  cudaFree(B.seg_row);
+  cudaFree(B.seg_begin);
+  cudaFree(B.seg_end);
+  cudaFree(B.seg_slot);
   B = DegreeBins();
 }
 
+namespace {
+
+// first arc of each (row, window) whose column is >= window * seg (rows sorted by column);
+// splits[r * (W + 1) + W] = end of row r
+__global__ void k_window_splits(const uint32_t* __restrict__ rows, uint64_t nrows, const uint64_t* __restrict__ off,
+                                const uint32_t* __restrict__ col, uint64_t seg, uint64_t W, uint64_t* __restrict__ splits) {
+  const uint64_t total = nrows * (W + 1);
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t r = t / (W + 1), w = t - r * (W + 1);
+    const uint32_t v = rows[r];
+    uint64_t lo = off[v], hi = off[v + 1];
+    if (w == W) {
+      lo = hi;
+    } else {
+      const uint64_t key = w * seg;
+      while (lo < hi) {
+        const uint64_t mid = (lo + hi) >> 1;
+        if ((uint64_t)col[mid] < key) lo = mid + 1;
+        else hi = mid;
+      }
+    }
+    splits[t] = lo;
+  }
+}
+
+// Window-split chunks of the rows above cta_min (bins 6 and 7), see DegreeBins.
+int build_segments(gre_graph g, DegreeBins& B, const uint64_t* off, const uint32_t* col) {
+  const uint64_t seg = B.sched.seg_window;
+  const uint64_t nrows = B.count[6] + B.count[7];
+  if (!seg || !nrows) return GRE_SUCCESS;
+  const uint64_t W = (g->n + seg - 1) / seg;
+  const uint32_t* rows = B.rows + B.start[6];  // bins 6 and 7 are contiguous
+  uint64_t* dsplits = nullptr;
+  GRE_CUDA(cudaMalloc(&dsplits, sizeof(uint64_t) * nrows * (W + 1)));
+  std::vector<uint64_t> sp(nrows * (W + 1));
+  k_window_splits<<<grid_for(nrows * (W + 1), 256), 256, 0, g->stream>>>(rows, nrows, off, col, seg, W, dsplits);
+  cudaError_t e = cudaMemcpyAsync(sp.data(), dsplits, sizeof(uint64_t) * sp.size(), cudaMemcpyDeviceToHost, g->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  cudaFree(dsplits);
+  if (e != cudaSuccess) return cuda_status(e, "window splits", __FILE__, __LINE__);
+  // the first arc of a row is its start: pieces of (row, window) of at most hub_chunk arcs; slots
+  // row-major (a row's pieces in window order), processing order window-major
+  const uint64_t piece = B.sched.hub_chunk;
+  std::vector<uint64_t> first(nrows + 1, 0);
+  for (uint64_t r = 0; r < nrows; ++r) {
+    uint64_t k = 0;
+    for (uint64_t w = 0; w < W; ++w) {
+      const uint64_t a0 = sp[r * (W + 1) + w], a1 = sp[r * (W + 1) + w + 1];
+      if (a1 > a0) k += (a1 - a0 + piece - 1) / piece;
+    }
+    first[r + 1] = first[r] + k;
+  }
+  const uint64_t nchunks = first[nrows];
+  std::vector<uint32_t> crow(nchunks);
+  std::vector<uint64_t> cbeg(nchunks), cend(nchunks), cslot(nchunks), next(first.begin(), first.end() - 1);
+  std::vector<uint32_t> hrows(nrows);
+  e = cudaMemcpy(hrows.data(), rows, sizeof(uint32_t) * nrows, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_status(e, "window rows", __FILE__, __LINE__);
+  uint64_t c = 0;
+  for (uint64_t w = 0; w < W; ++w)
+    for (uint64_t r = 0; r < nrows; ++r) {
+      const uint64_t a0 = sp[r * (W + 1) + w], a1 = sp[r * (W + 1) + w + 1];
+      for (uint64_t a = a0; a < a1; a += piece, ++c) {
+        crow[c] = hrows[r];
+        cbeg[c] = a;
+        cend[c] = a + piece < a1 ? a + piece : a1;
+        cslot[c] = next[r]++;
+      }
+    }
+  B.seg_nrows = nrows;
+  B.seg_nchunks = nchunks;
+  e = cudaMalloc(&B.seg_rows, sizeof(uint32_t) * nrows);
+  if (e == cudaSuccess) e = cudaMalloc(&B.seg_first, sizeof(uint64_t) * (nrows + 1));
+  if (e == cudaSuccess) e = cudaMalloc(&B.seg_row, sizeof(uint32_t) * (nchunks ? nchunks : 1));
+  if (e == cudaSuccess) e = cudaMalloc(&B.seg_begin, sizeof(uint64_t) * (nchunks ? nchunks : 1));
+  if (e == cudaSuccess) e = cudaMalloc(&B.seg_end, sizeof(uint64_t) * (nchunks ? nchunks : 1));
+  if (e == cudaSuccess) e = cudaMalloc(&B.seg_slot, sizeof(uint64_t) * (nchunks ? nchunks : 1));
+  if (e == cudaSuccess) e = cudaMemcpy(B.seg_rows, hrows.data(), sizeof(uint32_t) * nrows, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(B.seg_first, first.data(), sizeof(uint64_t) * (nrows + 1), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && nchunks) e = cudaMemcpy(B.seg_row, crow.data(), sizeof(uint32_t) * nchunks, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && nchunks) e = cudaMemcpy(B.seg_begin, cbeg.data(), sizeof(uint64_t) * nchunks, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && nchunks) e = cudaMemcpy(B.seg_end, cend.data(), sizeof(uint64_t) * nchunks, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && nchunks) e = cudaMemcpy(B.seg_slot, cslot.data(), sizeof(uint64_t) * nchunks, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_status(e, "window chunk upload", __FILE__, __LINE__);
+  // partial slots the row kernels need
+  if (nchunks > B.n_hub_chunks) B.n_hub_chunks = nchunks;
+  return GRE_SUCCESS;
+}
+
+
 // Groups the rows of `off` by bin under `sched` (replacing what B held).
-int build_bins(gre_graph g, DegreeBins& B, const uint64_t* off, const RowSchedule& sched) {
+int build_bins(gre_graph g, DegreeBins& B, const uint64_t* off, const uint32_t* col, const RowSchedule& sched) {
   free_bins(B);
   B.sched = sched;
   const uint64_t n = g->n;
@@ -177,6 +280,7 @@ int build_bins(gre_graph g, DegreeBins& B, const uint64_t* off, const RowSchedul
   cudaFree(iota);
   cudaFree(nsel);
   cudaFree(spans);
+  if (!st) st = build_segments(g, B, off, col);
   if (st) {
     free_bins(B);
     return st;
@@ -234,7 +338,7 @@ int probe(gre_graph g, const DegreeBins& B, const uint64_t* off, const uint32_t*
   return st;
 }
 
-int tune(gre_graph g, DegreeBins& B, const uint64_t* off, const uint32_t* col, RowSchedule* best) {
+int tune(gre_graph g, DegreeBins& B, const uint64_t* off, const uint32_t* col, bool sorted, RowSchedule* best) {
   double *x = nullptr, *y = nullptr;
   GRE_CUDA(cudaMalloc(&x, sizeof(double) * g->n));
   cudaError_t e = cudaMalloc(&y, sizeof(double) * g->n);
@@ -248,12 +352,28 @@ int tune(gre_graph g, DegreeBins& B, const uint64_t* off, const uint32_t* col, R
       cand.lane_arcs = lane_arcs;
       cand.cta_min = cta_min;
       float ms = 0;
-      st = build_bins(g, B, off, cand);
+      st = build_bins(g, B, off, col, cand);
       if (!st) st = probe(g, B, off, col, x, y, &ms);
       if (!st && ms < best_ms) {
         best_ms = ms;
         *best = cand;
       }
+    }
+  }
+  // source windows for the rows above cta_min, when the rows are sorted and the gathered
+  // values (8 bytes per vertex) outgrow a window of 64 MB (half the L2).  On RMAT-26 the windows
+  // measured no faster (the hub rows' gathers are bound by L2 request rate, not by misses), so
+  // one window size is tried, to keep the tuning short.
+  for (uint64_t window : {1ull << 23}) {
+    if (st || !sorted || g->n <= window) break;
+    RowSchedule cand = *best;
+    cand.seg_window = window;
+    float ms = 0;
+    st = build_bins(g, B, off, col, cand);
+    if (!st) st = probe(g, B, off, col, x, y, &ms);
+    if (!st && ms < best_ms) {
+      best_ms = ms;
+      *best = cand;
     }
   }
   cudaFree(x);
@@ -276,10 +396,24 @@ int ensure_bins(gre_graph g, bool in) {
   if (B.ready) return GRE_SUCCESS;
   const uint64_t* off = in ? g->roff : g->off;
   const uint32_t* col = in ? g->rcol : g->col;
+  const bool sorted = in && !g->symmetric() ? true : g->csr_sorted;  // the CSC is built sorted
   RowSchedule sched;  // default
+  if (const char* e = getenv("GRE_ROW_SCHEDULE")) {  // "lane_arcs,cta_min,hub_chunk,seg_window": a fixed schedule
+    unsigned long long a = 0, c = 0, h = 0, w = 0;
+    if (sscanf(e, "%llu,%llu,%llu,%llu", &a, &c, &h, &w) != 4 || a < 1 || a > 64 || c < 16 * a || h < c || h == 0) {
+      set_error("GRE_ROW_SCHEDULE must be lane_arcs,cta_min,hub_chunk,seg_window with 16*lane_arcs <= cta_min <= hub_chunk");
+      return GRE_INVALID_ARG;
+    }
+    sched.lane_arcs = (uint32_t)a;
+    sched.cta_min = c;
+    sched.hub_chunk = h;
+    sched.seg_window = sorted ? w : 0;
+    return build_bins(g, B, off, col, sched);
+  }
   if (tuning_enabled() && g->m >= kTuneMinArcs) {
     std::string key;
     GRE_CHECK(degree_key(g, off, &key));
+    key += sorted ? "sorted" : "unsorted";
     bool found = false;
     {
       std::lock_guard<std::mutex> lock(g_tuned_mu);
@@ -290,27 +424,29 @@ int ensure_bins(gre_graph g, bool in) {
       }
     }
     if (!found) {
-      GRE_CHECK(tune(g, B, off, col, &sched));
+      GRE_CHECK(tune(g, B, off, col, sorted, &sched));
       std::lock_guard<std::mutex> lock(g_tuned_mu);
       g_tuned[key] = sched;
     }
     if (B.ready && B.sched.lane_arcs == sched.lane_arcs && B.sched.cta_min == sched.cta_min &&
-        B.sched.hub_chunk == sched.hub_chunk)
+        B.sched.hub_chunk == sched.hub_chunk && B.sched.seg_window == sched.seg_window)
       return GRE_SUCCESS;  // the last candidate tried is the one kept
   }
-  return build_bins(g, B, off, sched);
+  return build_bins(g, B, off, col, sched);
 }
 
 }  // namespace gre
 
-extern "C" int gre_row_schedule(gre_graph g, int in, uint32_t* lane_arcs, uint64_t* cta_min, uint64_t* hub_chunk) {
+extern "C" int gre_row_schedule(gre_graph g, int in, uint32_t* lane_arcs, uint64_t* cta_min, uint64_t* hub_chunk,
+                                uint64_t* seg_window) {
   using namespace gre;
-  if (!g || !lane_arcs || !cta_min || !hub_chunk) return GRE_NULL;
+  if (!g || !lane_arcs || !cta_min || !hub_chunk || !seg_window) return GRE_NULL;
   GRE_CHECK(use_graph(g));
   GRE_CHECK(ensure_bins(g, in != 0));
   const DegreeBins& B = in ? g->bins_in : g->bins_out;
   *lane_arcs = B.sched.lane_arcs;
   *cta_min = B.sched.cta_min;
   *hub_chunk = B.sched.hub_chunk;
+  *seg_window = B.seg_nchunks ? B.sched.seg_window : 0;
   return GRE_SUCCESS;
 }

@@ -274,12 +274,8 @@ void destroy_graph(gre_graph g) {
   cudaFree(g->w32);
   cudaFree(g->w64);
   cudaFree(g->rw64);
-  for (DegreeBins* b : {&g->bins_in, &g->bins_out}) {
-    cudaFree(b->rows);
-    cudaFree(b->hub_chunk_row);
-    cudaFree(b->hub_chunk_begin);
-    cudaFree(b->hub_chunk_first);
-  }
+  free_bins(g->bins_in);
+  free_bins(g->bins_out);
   cudaFree(g->bc_chunks.rows);
   cudaFree(g->bc_chunks.chunk_row);
   cudaFree(g->bc_chunks.chunk_begin);
@@ -344,8 +340,32 @@ static int build_csc(gre_graph g) {
 }
 
 // Degrees, maxima and the CSC; called once the CSR is on the device.
+// warp per row: clears *sorted if a row's columns decrease somewhere
+__global__ void k_rows_sorted(uint64_t n, const uint64_t* __restrict__ off, const uint32_t* __restrict__ col,
+                              unsigned int* __restrict__ sorted) {
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31u;
+  bool ok = true;
+  for (uint64_t v = warp; v < n; v += nwarps)
+    for (uint64_t a = off[v] + lane; a + 1 < off[v + 1]; a += 32) ok = ok && col[a] <= col[a + 1];
+  if (!__all_sync(0xffffffffu, ok) && lane == 0) atomicAnd(sorted, 0u);
+}
+
 int finish_graph(gre_graph g) {
   const uint64_t n = g->n;
+  {
+    unsigned int* flag = nullptr;
+    GRE_CHECK(g->ws.get(WS_COUNTERS, 64, (void**)&flag));
+    const unsigned int one = 1;
+    GRE_CUDA(cudaMemcpyAsync(flag, &one, sizeof one, cudaMemcpyHostToDevice, g->stream));
+    k_rows_sorted<<<grid_for(n * 32, 256), 256, 0, g->stream>>>(n, g->off, g->col, flag);
+    GRE_LAUNCH_CHECK();
+    unsigned int h = 0;
+    GRE_CUDA(cudaMemcpyAsync(&h, flag, sizeof h, cudaMemcpyDeviceToHost, g->stream));
+    GRE_CUDA(cudaStreamSynchronize(g->stream));
+    g->csr_sorted = h != 0;
+  }
   GRE_CUDA(cudaMalloc(&g->outdeg, sizeof(uint32_t) * n));
   k_degree<<<grid_for(n, 256), 256, 0, g->stream>>>(n, g->off, g->outdeg);
   GRE_LAUNCH_CHECK();
@@ -393,13 +413,8 @@ static void drop_derived(gre_graph g) {
   if (g->indeg != g->outdeg) cudaFree(g->indeg);
   cudaFree(g->outdeg);
   g->indeg = g->outdeg = nullptr;
-  for (DegreeBins* b : {&g->bins_in, &g->bins_out}) {
-    cudaFree(b->rows);
-    cudaFree(b->hub_chunk_row);
-    cudaFree(b->hub_chunk_begin);
-    cudaFree(b->hub_chunk_first);
-    *b = DegreeBins();
-  }
+  free_bins(g->bins_in);
+  free_bins(g->bins_out);
   cudaFree(g->bc_chunks.rows);
   cudaFree(g->bc_chunks.chunk_row);
   cudaFree(g->bc_chunks.chunk_begin);

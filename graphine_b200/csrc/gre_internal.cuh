@@ -69,6 +69,10 @@ struct RowSchedule {
   uint32_t lane_arcs = 4;
   uint64_t cta_min = 4096;
   uint64_t hub_chunk = 65536;
+  // Rows above cta_min split at source windows of seg_window vertices (0: not split); needs
+  // rows sorted by column.  Their chunks run window after window, so the values gathered by
+  // all of them come from one window at a time, which stays in L2.
+  uint64_t seg_window = 0;
 };
 
 struct DegreeBins {
@@ -82,6 +86,17 @@ struct DegreeBins {
   uint64_t* hub_chunk_row = nullptr;   // per chunk: index into the multi-CTA bin
   uint64_t* hub_chunk_begin = nullptr; // per chunk: first arc
   uint64_t* hub_chunk_first = nullptr; // per multi-CTA row: first chunk id (size count+1)
+  // Window-split rows (sched.seg_window != 0): the rows above cta_min (bins 6 and 7).  Chunk c,
+  // in processing order (window-major), covers arcs [seg_begin[c], seg_end[c]) of vertex
+  // seg_row[c] and writes its partial sum to slot seg_slot[c]; row i of seg_rows adds slots
+  // seg_first[i] .. seg_first[i+1]-1 in order (its chunks in window order).
+  uint64_t seg_nrows = 0, seg_nchunks = 0;
+  uint32_t* seg_rows = nullptr;
+  uint64_t* seg_first = nullptr;
+  uint32_t* seg_row = nullptr;
+  uint64_t* seg_begin = nullptr;
+  uint64_t* seg_end = nullptr;
+  uint64_t* seg_slot = nullptr;
 };
 
 // Rows longer than `ch` arcs split into fixed chunks of `ch` arcs from the row start.  Partial
@@ -113,6 +128,7 @@ struct gre_graph_s {
   uint64_t* rarc = nullptr;  // CSC slot -> CSR arc id (built on demand)
   uint32_t* outdeg = nullptr;
   uint32_t* indeg = nullptr;  // aliases outdeg when symmetric
+  bool csr_sorted = false;    // every CSR row lists its columns in increasing order (the CSC always does)
   // weights
   uint32_t* w32 = nullptr;
   double w32_mean = -1.0;  // mean of w32, computed on first use (-1: unknown)
@@ -309,6 +325,7 @@ inline void stats_record(gre_stats* st, uint64_t active) {
 
 // Degree bins of the CSC (in = true) or CSR; built once per graph.
 int ensure_bins(gre_graph g, bool in);
+void free_bins(DegreeBins& B);
 // CSC slot -> CSR arc map; built once per graph.
 int ensure_rarc(gre_graph g);
 // Undirected edge count with both endpoints in a reached set (Graph500 TEPS numerator).

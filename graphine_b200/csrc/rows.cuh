@@ -105,6 +105,30 @@ __global__ void __launch_bounds__(kCta) k_rows_chunks(const uint32_t* __restrict
   }
 }
 
+// Window-split rows (DegreeBins::seg_*): CTA per chunk in processing order, partial sums by slot.
+template <class Gather>
+__global__ void __launch_bounds__(kCta) k_rows_seg(const uint32_t* __restrict__ row, const uint64_t* __restrict__ begin,
+                                                   const uint64_t* __restrict__ end, const uint64_t* __restrict__ slot,
+                                                   uint64_t nchunks, Gather gat, double* __restrict__ partial) {
+  __shared__ double smem[kCta / 32];
+  for (uint64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    const uint32_t v = row[c];
+    double acc = strided_sum<kCta>(gat, v, begin[c], end[c], threadIdx.x);
+    acc = block_sum(acc, smem);
+    if (threadIdx.x == 0) partial[slot[c]] = acc;
+  }
+}
+
+template <class Finish>
+__global__ void k_rows_seg_finish(const uint32_t* __restrict__ rows, uint64_t count, const uint64_t* __restrict__ first,
+                                  const double* __restrict__ partial, Finish fin) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count; i += (uint64_t)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (uint64_t c = first[i]; c < first[i + 1]; ++c) s += partial[c];
+    fin(rows[i], s);
+  }
+}
+
 template <class Finish>
 __global__ void k_rows_chunk_finish(const uint32_t* __restrict__ rows, uint64_t count, const uint64_t* __restrict__ first,
                                     const double* __restrict__ partial, Finish fin) {
@@ -126,6 +150,13 @@ int reduce_rows(const DegreeBins& B, const uint64_t* off, Gather gat, Finish fin
   if (B.count[3]) k_rows_lanes<8><<<grid(B.count[3] * 8), 256, 0, s>>>(r + B.start[3], B.count[3], off, gat, fin);
   if (B.count[4]) k_rows_lanes<16><<<grid(B.count[4] * 16), 256, 0, s>>>(r + B.start[4], B.count[4], off, gat, fin);
   if (B.count[5]) k_rows_lanes<32><<<grid(B.count[5] * 32), 256, 0, s>>>(r + B.start[5], B.count[5], off, gat, fin);
+  if (B.seg_nchunks) {  // rows above cta_min, window by window
+    k_rows_seg<<<grid_for(B.seg_nchunks * kCta, kCta, 8), kCta, 0, s>>>(B.seg_row, B.seg_begin, B.seg_end, B.seg_slot,
+                                                                         B.seg_nchunks, gat, partial);
+    k_rows_seg_finish<<<grid_for(B.seg_nrows, 128, 4), 128, 0, s>>>(B.seg_rows, B.seg_nrows, B.seg_first, partial, fin);
+    GRE_LAUNCH_CHECK();
+    return GRE_SUCCESS;
+  }
   if (B.count[6]) k_rows_cta<<<grid_for(B.count[6] * kCta, kCta, 8), kCta, 0, s>>>(r + B.start[6], B.count[6], off, gat, fin);
   if (B.count[7]) {
     k_rows_chunks<<<grid_for(B.n_hub_chunks * kCta, kCta, 8), kCta, 0, s>>>(r + B.start[7], B.hub_chunk_row, B.hub_chunk_begin,

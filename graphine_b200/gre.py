@@ -110,7 +110,7 @@ def lib() -> C.CDLL:
             "gre_graph_free": (I32, [P]),
             "gre_graph_reorder": (I32, [P]),
             "gre_graph_info": (I32, [P, C.POINTER(U64), C.POINTER(U64), C.POINTER(U32)]),
-            "gre_row_schedule": (I32, [P, I32, C.POINTER(U32), C.POINTER(U64), C.POINTER(U64)]),
+            "gre_row_schedule": (I32, [P, I32, C.POINTER(U32), C.POINTER(U64), C.POINTER(U64), C.POINTER(U64)]),
             "gre_graph_outdegree": (I32, [P, P]),
             "gre_graph_csr": (I32, [P, P, P]),
             "gre_graph_set_weights_u32": (I32, [P, P]),
@@ -300,10 +300,11 @@ class Graph:
         return out
 
     def row_schedule(self, incoming: bool = True):
-        """(lane_arcs, cta_min, hub_chunk) of the degree bins, tuned on first use."""
-        a, c, h = C.c_uint32(), C.c_uint64(), C.c_uint64()
-        _check(lib().gre_row_schedule(self._h, int(incoming), C.byref(a), C.byref(c), C.byref(h)), "gre_row_schedule")
-        return a.value, c.value, h.value
+        """(lane_arcs, cta_min, hub_chunk, seg_window) of the degree bins, tuned on first use."""
+        a, c, h, w = C.c_uint32(), C.c_uint64(), C.c_uint64(), C.c_uint64()
+        _check(lib().gre_row_schedule(self._h, int(incoming), C.byref(a), C.byref(c), C.byref(h), C.byref(w)),
+               "gre_row_schedule")
+        return a.value, c.value, h.value, w.value
 
     def csr(self):
         off = np.empty(self.n + 1, dtype=np.uint64)

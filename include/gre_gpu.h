@@ -128,11 +128,13 @@ int gre_graph_reorder(gre_graph g);
 int gre_graph_info(gre_graph g, uint64_t* n, uint64_t* m, uint32_t* flags);
 /* Threads-per-row schedule of the graph's in-arc (in != 0) or out-arc rows, chosen on first use
  * by the autotuner from the degree distribution (GRE_TUNE=0 in the environment: the default
- * 4 / 4096 / 65536).  Rows of up to lane_arcs * 2^b arcs get 2^b lanes (b < 5), then a warp up
- * to cta_min arcs, a CTA up to hub_chunk arcs, and chunks of hub_chunk arcs beyond.  Replaces
- * the reference's one-thread-per-vertex compute loop (Engine.hpp:592-625), which has no
- * such knob. */
-int gre_row_schedule(gre_graph g, int in, uint32_t* lane_arcs, uint64_t* cta_min, uint64_t* hub_chunk);
+ * 4 / 4096 / 65536 / 0).  Rows of up to lane_arcs * 2^b arcs get 2^b lanes (b < 5), then a warp
+ * up to cta_min arcs, a CTA up to hub_chunk arcs, and chunks of hub_chunk arcs beyond; with
+ * seg_window != 0 the rows above cta_min are instead cut at source windows of seg_window
+ * vertices and processed window by window.  Replaces the reference's one-thread-per-vertex
+ * compute loop (Engine.hpp:592-625), which has no such knob. */
+int gre_row_schedule(gre_graph g, int in, uint32_t* lane_arcs, uint64_t* cta_min, uint64_t* hub_chunk,
+                     uint64_t* seg_window);
 /* getOutdegree for every vertex (DistributedGraph.hpp:178-180). */
 int gre_graph_outdegree(gre_graph g, uint32_t* outdeg);
 /* Copy the CSR back (row_off[n+1], col[m]) in caller ids; its arc order is the order every

@@ -391,15 +391,42 @@ def test_relabelled_explicit_weights_match_plain(when):
     np.testing.assert_array_equal(d2, d0.reshape(len(roots), n)[2])
 
 
+@pytest.mark.parametrize("schedule", ["1,16,64,0", "2,32,256,1024", "8,128,4096,4096", "4,4096,65536,0", "2,32,64,512"])
+@pytest.mark.parametrize("directed", [False, True], ids=["sym", "dir"])
+def test_forced_row_schedules_match_oracle(monkeypatch, schedule, directed):
+    """Every row kernel (lanes, CTA, fixed chunks, source-window chunks) gives the oracle's sums."""
+    n, off, col = G.rmat_host(14, 16, 42, not directed)
+    R = O.Restatement.from_csr(n, off, col)
+    monkeypatch.setenv("GRE_ROW_SCHEDULE", schedule)
+    g = G.Graph.from_csr(n, off, col, dir=G.InOut, symmetric=not directed, reorder=True)
+    sched = tuple(int(x) for x in schedule.split(","))
+    got = g.row_schedule()
+    assert got[:3] == sched[:3] and got[3] in (0, sched[3])  # no window cut when no row is above cta_min
+    ref, _ = R.pagerank(1, 0.85, 20)
+    pr, _ = G.pagerank(g, G.PR_ITER, 0.85, 20)
+    assert rel_l1(pr, ref) <= TOL
+    if not directed:
+        lab, _ = G.cc(g)
+        np.testing.assert_array_equal(lab, R.cc()[0])
+    w = np.exp(np.random.default_rng(3).standard_normal(len(col)))
+    g.set_weights_f64(w)
+    r1, _, _ = G.pagerank_weighted(g, 0.85, None, tol=1e-14, max_iters=500)
+    monkeypatch.setenv("GRE_ROW_SCHEDULE", "4,4096,65536,0")
+    g0 = G.Graph.from_csr(n, off, col, dir=G.InOut, symmetric=not directed, reorder=True)
+    g0.set_weights_f64(w)
+    r0, _, _ = G.pagerank_weighted(g0, 0.85, None, tol=1e-14, max_iters=500)
+    assert rel_l1(r1, r0) <= 1e-12
+
+
 def test_autotuned_row_schedule_keeps_results(monkeypatch):
     """The tuner picks a schedule from its candidates; results equal the default schedule's
     (bit-exact for BFS/CC, FP64 sums within a few ulps: only the association order differs)."""
     g = G.Graph.rmat(20, 16, 77, True, reorder=True)
-    lane_arcs, cta_min, hub = g.row_schedule()
+    lane_arcs, cta_min, hub, _ = g.row_schedule()
     assert lane_arcs in (2, 4, 8) and cta_min in (1024, 4096, 16384) and hub == 65536
     monkeypatch.setenv("GRE_TUNE", "0")
     g0 = G.Graph.rmat(20, 16, 77, True, reorder=True)
-    assert g0.row_schedule() == (4, 4096, 65536)
+    assert g0.row_schedule() == (4, 4096, 65536, 0)
     pr, _ = G.pagerank(g, G.PR_ITER, 0.85, 20)
     pr0, _ = G.pagerank(g0, G.PR_ITER, 0.85, 20)
     assert rel_l1(pr, pr0) <= 1e-13
