@@ -1,0 +1,98 @@
+"""Degenerate inputs on every fast path and engine plugin, against the oracle restatement:
+a graph without arcs, a single vertex, self loops and parallel arcs only, isolated sources,
+sources repeated in one batch, a batch of exactly 64 / 65 sources (one full word and one bit
+of the next), and a union with an empty member."""
+import numpy as np
+import pytest
+
+import graphine_b200.gre as G
+import oracle as O
+from conftest import rel_l1
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-9
+REORDER = pytest.mark.parametrize("reorder", [False, True], ids=["plain", "relabelled"])
+
+
+def csr(n, edges):
+    src = np.array([e[0] for e in edges], dtype=np.int64)
+    dst = np.array([e[1] for e in edges], dtype=np.uint32)
+    order = np.argsort(src, kind="stable")
+    off = np.zeros(n + 1, np.uint64)
+    np.add.at(off, src + 1, 1)
+    return np.cumsum(off).astype(np.uint64), dst[order]
+
+
+def check_all(n, off, col, roots, reorder, wseed=5):
+    g = G.Graph.from_csr(n, off, col, dir=G.InOut, symmetric=True, reorder=reorder)
+    g.set_weights_hash(wseed)
+    R = O.Restatement.from_csr(n, off, col)
+    roots = np.asarray(roots, np.uint32)
+    pr_ref, _ = R.pagerank(1, 0.85, 20)
+    assert rel_l1(G.pagerank(g, G.PR_ITER, 0.85, 20)[0], pr_ref) <= TOL
+    assert rel_l1(G.vc_pagerank(g, G.PR_ITER, 20)[0], pr_ref) <= TOL
+    lv_ref = R.bfs_many(roots)
+    np.testing.assert_array_equal(G.bfs(g, roots)[0].reshape(len(roots), n), lv_ref)
+    np.testing.assert_array_equal(G.msbfs(g, roots)[0].reshape(len(roots), n), lv_ref)
+    np.testing.assert_array_equal(G.vc_bfs(g, int(roots[0]), G.In)[1], lv_ref[0])
+    d_ref = R.sssp_many(roots, wseed)
+    np.testing.assert_array_equal(G.sssp(g, roots)[0].reshape(len(roots), n), d_ref)
+    np.testing.assert_array_equal(G.vc_sssp(g, int(roots[0]))[0], d_ref[0])
+    lab_ref, _ = R.cc()
+    np.testing.assert_array_equal(G.cc(g)[0], lab_ref)
+    np.testing.assert_array_equal(G.vc_cc(g)[0], lab_ref)
+    bc_ref, _ = R.bc(roots)
+    b1, _ = G.bc(g, roots, batched=False)
+    b2, _ = G.bc(g, roots, batched=True)
+    np.testing.assert_array_equal(b1, b2)
+    assert rel_l1(b1, bc_ref) <= TOL or np.abs(b1 - bc_ref).max() <= 1e-12
+    ppr_ref = R.ppr(roots[:3], 0.85, 20)
+    assert rel_l1(G.ppr(g, roots[:3], 0.85, 20)[0], ppr_ref.ravel()) <= TOL
+    return g
+
+
+@REORDER
+def test_graph_without_arcs(reorder):
+    n = 5
+    off = np.zeros(n + 1, np.uint64)
+    col = np.zeros(0, np.uint32)
+    check_all(n, off, col, [0, 3], reorder)
+
+
+@REORDER
+def test_single_vertex_with_self_loop_and_parallel_arcs(reorder):
+    check_all(1, *csr(1, [(0, 0), (0, 0)]), [0], reorder)
+
+
+@REORDER
+def test_isolated_sources_and_repeated_sources(reorder):
+    n = 9
+    edges = [(0, 1), (1, 0), (1, 2), (2, 1), (2, 2), (5, 6), (6, 5), (5, 6), (6, 5)]
+    check_all(n, *csr(n, edges), [3, 0, 0, 8, 5], reorder)
+
+
+@pytest.mark.parametrize("k", [64, 65])
+def test_full_and_spilling_source_words(k):
+    n, off, col = G.rmat_host(10, 8, 21, True)
+    roots = G.sample_sources(off, k, 3)
+    check_all(n, off, col, roots, True)
+
+
+def test_union_with_an_empty_member():
+    parts = [(3, *csr(3, [])), (4, *csr(4, [(0, 1), (1, 0), (2, 3), (3, 2)])), (1, *csr(1, []))]
+    gs = [G.Graph.from_csr(n, o, c, dir=G.InOut, symmetric=True) for n, o, c in parts]
+    u, voff = G.Graph.union(gs)
+    assert list(voff) == [0, 3, 7, 8]
+    lv, _ = G.bfs_multiroot(u, [1, 3 + 2, 7])
+    np.testing.assert_array_equal(lv, [-1, 0, -1, -1, -1, 0, 1, 0])
+    lab, _ = G.cc(u)
+    np.testing.assert_array_equal(lab, [0, 1, 2, 3, 3, 5, 5, 7])
+
+
+def test_zero_sources_and_zero_seeds():
+    n, off, col = G.rmat_host(8, 8, 2, True)
+    g = G.Graph.from_csr(n, off, col, dir=G.InOut, symmetric=True)
+    b, _ = G.bc(g, np.zeros(0, np.uint32))
+    assert not b.any()
+    out, _ = G.ppr(g, np.zeros(0, np.uint32))
+    assert out.size == 0
