@@ -289,20 +289,22 @@ int bfs_levels(gre_graph g, const uint32_t* droots, uint32_t nroots, int32_t* le
 }
 
 // Undirected edges with a reached endpoint: sum over reached v of outdeg(v) / 2 (symmetric).
-__global__ void k_reached_degree(uint64_t n, const int32_t* __restrict__ level, const uint32_t* __restrict__ deg,
+// sum of the degrees of reached vertices over `rows` level arrays of n entries each
+__global__ void k_reached_degree(uint64_t n, uint64_t rows, const int32_t* __restrict__ level, const uint32_t* __restrict__ deg,
                                  unsigned long long* __restrict__ out) {
   unsigned long long s = 0;
-  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x)
-    if (level[v] >= 0) s += deg[v];
+  const uint64_t total = n * rows;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x)
+    if (level[i] >= 0) s += deg[i % n];
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   if ((threadIdx.x & 31u) == 0 && s) atomicAdd(out, s);
 }
 
-int count_reached_edges(gre_graph g, const int32_t* level, uint64_t* edges) {
+int count_reached_edges(gre_graph g, const int32_t* level, uint64_t* edges, uint64_t rows) {
   unsigned long long* c;
   GRE_CHECK(ws_array(g, WS_COUNTERS, 4, &c));
   GRE_CUDA(cudaMemsetAsync(c, 0, 8, g->stream));
-  k_reached_degree<<<grid_for(g->n, 256), 256, 0, g->stream>>>(g->n, level, g->outdeg, c);
+  k_reached_degree<<<grid_for(g->n * rows, 256), 256, 0, g->stream>>>(g->n, rows, level, g->outdeg, c);
   unsigned long long h = 0;
   GRE_CUDA(cudaMemcpyAsync(&h, c, 8, cudaMemcpyDeviceToHost, g->stream));
   GRE_CUDA(cudaStreamSynchronize(g->stream));
@@ -505,11 +507,7 @@ int gre_msbfs(gre_graph g, const uint32_t* srcs, uint32_t nsrc, int32_t* levels,
     }
   }
   uint64_t edges = 0;
-  for (uint32_t i = 0; i < nsrc; ++i) {
-    uint64_t e = 0;
-    GRE_CHECK(count_reached_edges(g, dl + (uint64_t)i * n, &e));
-    edges += e;
-  }
+  GRE_CHECK(count_reached_edges(g, dl, &edges, nsrc));  // all sources in one pass
   GRE_CHECK(perm_out_end(g, dl, dfinal, nsrc, 4));
   GRE_CHECK(finish_output(g, levels, dfinal, (uint64_t)nsrc * n));
   GRE_CHECK(timer.stop(st));

@@ -329,7 +329,7 @@ void free_bins(DegreeBins& B);
 // CSC slot -> CSR arc map; built once per graph.
 int ensure_rarc(gre_graph g);
 // Undirected edge count with both endpoints in a reached set (Graph500 TEPS numerator).
-int count_reached_edges(gre_graph g, const int32_t* level, uint64_t* edges);
+int count_reached_edges(gre_graph g, const int32_t* level, uint64_t* edges, uint64_t rows = 1);
 // Direction-optimising BFS levels from device roots (uses slots WS_A..WS_G, WS_COUNTERS, WS_CUB).
 int bfs_levels(gre_graph g, const uint32_t* droots, uint32_t nroots, int32_t* level, gre_stats* st, bool record);
 
