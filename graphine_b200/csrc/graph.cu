@@ -650,6 +650,12 @@ int gre_graph_load(const char* prefix, uint32_t flags, int device, gre_graph* ou
   return device_ingest(prefix, flags, device, out);
 }
 
+int gre_graph_load_parts(const char* prefix, uint32_t nparts, uint32_t flags, int device, gre_graph* out) {
+  if (!prefix || !out) return GRE_NULL;
+  clear_error();
+  return device_ingest_parts(prefix, nparts, flags, device, out);
+}
+
 int gre_graph_from_edges(uint64_t n, uint64_t m, const uint32_t* src, const uint32_t* dst, uint32_t flags, int device,
                          gre_graph* out) {
   if (!out || (m && (!src || !dst))) return GRE_NULL;

@@ -269,6 +269,7 @@ struct GraphGuard {
 };
 // <prefix>.meta + <prefix>.edges.<i> parsed on the device (ingest.cu).
 int device_ingest(const char* prefix, uint32_t flags, int device, gre_graph* out);
+int device_ingest_parts(const char* prefix, uint32_t nparts, uint32_t flags, int device, gre_graph* out);
 
 void launch_count_add(long long k);
 

@@ -253,34 +253,32 @@ int ingest_file(gre_graph g, Ingest& in, const std::string& name, uint64_t chunk
 
 }  // namespace
 
-int device_ingest(const char* prefix, uint32_t flags, int device, gre_graph* out) {
-  uint64_t nv = 0, ne = 0;
-  {
-    const std::string meta = std::string(prefix) + ".meta";
-    FILE* f = fopen(meta.c_str(), "r");
-    if (!f) {
-      set_error("cannot open %s", meta.c_str());
-      return GRE_IO_ERROR;
-    }
-    unsigned long long a = 0, b = 0;
-    const int k = fscanf(f, "%llu %llu", &a, &b);
-    fclose(f);
-    if (k != 2) {
-      set_error("%s: expected \"n m\"", meta.c_str());
-      return GRE_IO_ERROR;
-    }
-    if (a == 0 || a > 0xffffffffull) {
-      set_error("%s: vertex count %llu out of range", meta.c_str(), a);
-      return GRE_INVALID_ARG;
-    }
-    nv = a;
-    ne = b;
+namespace {
+
+int read_meta(const char* prefix, uint64_t* nv, uint64_t* ne) {
+  const std::string meta = std::string(prefix) + ".meta";
+  FILE* f = fopen(meta.c_str(), "r");
+  if (!f) {
+    set_error("cannot open %s", meta.c_str());
+    return GRE_IO_ERROR;
   }
-  gre_graph g = nullptr;
-  GRE_CHECK(new_graph(device, flags, &g));
-  GraphGuard guard{g};
-  Ingest in;
-  const uint64_t chunk = chunk_bytes();
+  unsigned long long a = 0, b = 0;
+  const int k = fscanf(f, "%llu %llu", &a, &b);
+  fclose(f);
+  if (k != 2) {
+    set_error("%s: expected \"n m\"", meta.c_str());
+    return GRE_IO_ERROR;
+  }
+  if (a == 0 || a > 0xffffffffull) {
+    set_error("%s: vertex count %llu out of range", meta.c_str(), a);
+    return GRE_INVALID_ARG;
+  }
+  *nv = a;
+  *ne = b;
+  return GRE_SUCCESS;
+}
+
+int alloc_ingest(gre_graph g, Ingest& in, uint64_t chunk, uint64_t ne) {
   GRE_CUDA(cudaHostAlloc((void**)&in.pin[0], chunk + 1, cudaHostAllocDefault));
   GRE_CUDA(cudaHostAlloc((void**)&in.pin[1], chunk + 1, cudaHostAllocDefault));
   GRE_CUDA(cudaMalloc(&in.dbuf, chunk + 1));
@@ -288,20 +286,13 @@ int device_ingest(const char* prefix, uint32_t flags, int device, gre_graph* out
   GRE_CUDA(cudaMalloc(&in.parsed, sizeof(uint64_t) * (chunk + 1)));
   GRE_CUDA(cudaMalloc(&in.counters, sizeof(unsigned long long) * 3));
   GRE_CUDA(cudaMemsetAsync(in.counters + 2, 0xff, sizeof(unsigned long long), g->stream));
-  GRE_CHECK(in.reserve(ne ? ne : 1024, g->stream));
-  uint64_t line0 = 0;
-  for (int i = 0;; ++i) {
-    const std::string name = std::string(prefix) + ".edges." + std::to_string(i);
-    bool missing = false;
-    const int st = ingest_file(g, in, name, chunk, nv, &line0, &missing);
-    if (st) return st;
-    if (missing) {
-      if (i > 0) break;  // the files are .edges.0 .. .edges.<P-1>
-      set_error("cannot open %s", name.c_str());
-      return GRE_IO_ERROR;
-    }
-  }
-  // CSR: stable sort by source keeps file order within a source (GraphInCSR::build)
+  return in.reserve(ne ? ne : 1024, g->stream);
+}
+
+// The edge list (packed source << 32 | target, in file order) -> CSR of g: a stable sort by
+// source keeps file order within a source (GraphInCSR::build); then relabelling and the
+// derived arrays.
+int finish_ingest(gre_graph g, Ingest& in, uint64_t nv, uint32_t flags) {
   const uint64_t m = in.m;
   g->n = nv;
   g->m = m;
@@ -346,7 +337,113 @@ int device_ingest(const char* prefix, uint32_t flags, int device, gre_graph* out
     std::swap(done.tmp, in.tmp);
   }
   if (flags & GRE_GRAPH_REORDER) GRE_CHECK(reorder_graph(g));
-  GRE_CHECK(finish_graph(g));
+  return finish_graph(g);
+}
+
+// (source, target) pairs of 64-bit vertex ids -> packed 32-bit pairs; ids not below n flag
+// GRE_INVALID_ARG with the pair index (the first bad pair in file order decides).
+__global__ void k_pack_pairs(const unsigned long long* __restrict__ pairs, uint64_t count, uint64_t pair0, uint64_t nv,
+                             uint64_t* __restrict__ out, unsigned long long* __restrict__ first_err) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count; i += (uint64_t)gridDim.x * blockDim.x) {
+    const unsigned long long u = pairs[2 * i], v = pairs[2 * i + 1];
+    if (u >= nv || v >= nv) {
+      atomicMin(first_err, (unsigned long long)(((pair0 + i) << 4) | (uint64_t)GRE_INVALID_ARG));
+      out[i] = 0;
+    } else {
+      out[i] = (u << 32) | v;
+    }
+  }
+}
+
+}  // namespace
+
+int device_ingest(const char* prefix, uint32_t flags, int device, gre_graph* out) {
+  uint64_t nv = 0, ne = 0;
+  GRE_CHECK(read_meta(prefix, &nv, &ne));
+  gre_graph g = nullptr;
+  GRE_CHECK(new_graph(device, flags, &g));
+  GraphGuard guard{g};
+  Ingest in;
+  const uint64_t chunk = chunk_bytes();
+  GRE_CHECK(alloc_ingest(g, in, chunk, ne));
+  uint64_t line0 = 0;
+  for (int i = 0;; ++i) {
+    const std::string name = std::string(prefix) + ".edges." + std::to_string(i);
+    bool missing = false;
+    const int st = ingest_file(g, in, name, chunk, nv, &line0, &missing);
+    if (st) return st;
+    if (missing) {
+      if (i > 0) break;  // the files are .edges.0 .. .edges.<P-1>
+      set_error("cannot open %s", name.c_str());
+      return GRE_IO_ERROR;
+    }
+  }
+  GRE_CHECK(finish_ingest(g, in, nv, flags));
+  *out = guard.release();
+  return GRE_SUCCESS;
+}
+
+// The reference's saved partitions (GraphIngress::loadEdgePartitions, GraphIngress.hpp:
+// 1024-1071): <prefix>.part.<P>.<r> holds rank r's edges as binary (vid_t, vid_t) pairs.  One
+// GPU holds every rank's part: the P files are read in rank order into one edge list (the
+// .outdegree and .scatterMap files only serve the rank exchange and are not needed).
+int device_ingest_parts(const char* prefix, uint32_t nparts, uint32_t flags, int device, gre_graph* out) {
+  uint64_t nv = 0, ne = 0;
+  GRE_CHECK(read_meta(prefix, &nv, &ne));
+  if (nparts == 0) {
+    set_error("gre_graph_load_parts: zero parts");
+    return GRE_INVALID_ARG;
+  }
+  gre_graph g = nullptr;
+  GRE_CHECK(new_graph(device, flags, &g));
+  GraphGuard guard{g};
+  Ingest in;
+  const uint64_t chunk = (chunk_bytes() / 16) * 16 ? (chunk_bytes() / 16) * 16 : 16;  // whole pairs
+  GRE_CHECK(alloc_ingest(g, in, chunk, ne));
+  uint64_t pair0 = 0;
+  for (uint32_t r = 0; r < nparts; ++r) {
+    const std::string name = std::string(prefix) + ".part." + std::to_string(nparts) + "." + std::to_string(r);
+    FILE* f = fopen(name.c_str(), "rb");
+    if (!f) {
+      set_error("cannot open %s", name.c_str());
+      return GRE_IO_ERROR;
+    }
+    int st = GRE_SUCCESS;
+    const uint64_t file_pair0 = pair0;
+    for (;;) {
+      const size_t got = fread(in.pin[0], 1, chunk, f);
+      if (got % 16) {
+        set_error("%s: size is not a multiple of 16 bytes (vid_t pairs)", name.c_str());
+        st = GRE_IO_ERROR;
+        break;
+      }
+      const uint64_t cnt = got / 16;
+      if (cnt) {
+        cudaError_t e = cudaMemcpyAsync(in.dbuf, in.pin[0], got, cudaMemcpyHostToDevice, g->stream);
+        if (e == cudaSuccess) st = in.reserve(in.m + cnt, g->stream);
+        if (e == cudaSuccess && !st) {
+          k_pack_pairs<<<grid_for(cnt, 256), 256, 0, g->stream>>>((const unsigned long long*)in.dbuf, cnt, pair0, nv, in.edges + in.m,
+                                                                  in.counters + 2);
+          unsigned long long bad = 0;
+          e = cudaMemcpyAsync(&bad, in.counters + 2, sizeof bad, cudaMemcpyDeviceToHost, g->stream);
+          if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+          if (e == cudaSuccess && bad != ~0ull) {
+            set_error("%s: pair %llu has a vertex id not below n = %llu", name.c_str(), (unsigned long long)((bad >> 4) - file_pair0),
+                      (unsigned long long)nv);
+            st = GRE_INVALID_ARG;
+          }
+        }
+        if (e != cudaSuccess && !st) st = cuda_status(e, "partition read", __FILE__, __LINE__);
+        if (st) break;
+        in.m += cnt;
+        pair0 += cnt;
+      }
+      if (got < chunk) break;
+    }
+    fclose(f);
+    if (st) return st;
+  }
+  GRE_CHECK(finish_ingest(g, in, nv, flags));
   *out = guard.release();
   return GRE_SUCCESS;
 }

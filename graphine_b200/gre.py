@@ -103,6 +103,7 @@ def lib() -> C.CDLL:
             "gre_device_count": (I32, [C.POINTER(I32)]),
             "gre_launch_count": (U64, []),
             "gre_graph_load": (I32, [C.c_char_p, U32, I32, C.POINTER(P)]),
+            "gre_graph_load_parts": (I32, [C.c_char_p, U32, U32, I32, C.POINTER(P)]),
             "gre_graph_from_edges": (I32, [U64, U64, P, P, U32, I32, C.POINTER(P)]),
             "gre_graph_from_csr": (I32, [U64, U64, P, P, U32, I32, C.POINTER(P)]),
             "gre_graph_rmat": (I32, [U32, U32, U64, I32, I32, C.POINTER(P)]),
@@ -227,6 +228,15 @@ class Graph:
         return cls(h.value)
 
     load = ingress
+
+    @classmethod
+    def load_parts(cls, prefix: str, nparts: int, dir: int = Out, symmetric: bool = False, device: int = 0,
+                   reorder: bool = False) -> "Graph":
+        """The reference's saved partitions <prefix>.part.<nparts>.<r> merged into one graph."""
+        h = C.c_void_p()
+        flags = dir | (SYMMETRIC if symmetric else 0) | (REORDER if reorder else 0)
+        _check(lib().gre_graph_load_parts(prefix.encode(), nparts, flags, device, C.byref(h)), "gre_graph_load_parts")
+        return cls(h.value)
 
     @classmethod
     def from_edges(cls, n: int, src, dst, dir: int = Out, symmetric: bool = False, device: int = 0,

@@ -102,6 +102,13 @@ uint64_t gre_launch_count(void);
  * (Graph/DistributedGraph.hpp:153-172; GraphIngress.hpp:76-304,323-328,511-723).
  * `flags` = gre_dir | gre_graph_flags.  Arc order: source-major, file order within a source. */
 int gre_graph_load(const char* prefix, uint32_t flags, int device, gre_graph* out);
+/* The reference's saved edge partitions (GraphIngress::loadEdgePartitions,
+ * GraphIngress.hpp:1024-1071): <prefix>.meta plus <prefix>.part.<nparts>.<r>, r < nparts, each a
+ * binary array of (uint64 source, uint64 target) pairs as an np = nparts run wrote them.  All
+ * parts are merged into one graph (rank order, file order within a rank); the .outdegree and
+ * .scatterMap files are not read (they only serve the exchange between ranks).  Flags as for
+ * gre_graph_load. */
+int gre_graph_load_parts(const char* prefix, uint32_t nparts, uint32_t flags, int device, gre_graph* out);
 /* GraphInCSR::build / rbuild from an edge list in input order (LocalGraph.hpp:66-156). */
 int gre_graph_from_edges(uint64_t n, uint64_t m, const uint32_t* src, const uint32_t* dst,
                          uint32_t flags, int device, gre_graph* out);

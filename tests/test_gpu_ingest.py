@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 
 import graphine_b200.gre as G
+import oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -119,3 +120,48 @@ def test_rmat_text_round_trip_relabelled():
     o2, c2 = g.csr()
     np.testing.assert_array_equal(o2, off)
     np.testing.assert_array_equal(c2, col)
+
+
+def write_parts(td, n, parts):
+    p = os.path.join(td, "p")
+    open(p + ".meta", "w").write(f"{n} {sum(len(x) for x in parts)}\n")
+    for r, pairs in enumerate(parts):
+        np.asarray(pairs, dtype=np.uint64).reshape(-1, 2).tofile(p + f".part.{len(parts)}.{r}")
+    return p
+
+
+@pytest.mark.parametrize("chunk", [None, "64"])
+def test_saved_partitions_merge_in_rank_order(monkeypatch, chunk):
+    if chunk:
+        monkeypatch.setenv("GRE_INGEST_CHUNK", chunk)
+    n, off, col = G.rmat_host(12, 8, 4, True)
+    src = np.repeat(np.arange(n, dtype=np.int64), np.diff(off.astype(np.int64)))
+    rank = np.random.default_rng(1).integers(0, 3, len(col))  # an arbitrary edge cut
+    parts = [np.stack([src[rank == r], col[rank == r].astype(np.int64)], axis=1) for r in range(3)]
+    with tempfile.TemporaryDirectory() as td:
+        g = G.Graph.load_parts(write_parts(td, n, parts), 3, G.InOut, symmetric=True)
+    allp = np.concatenate(parts)
+    order = np.argsort(allp[:, 0], kind="stable")
+    o2, c2 = g.csr()
+    np.testing.assert_array_equal(o2, off)
+    np.testing.assert_array_equal(c2, allp[order, 1].astype(np.uint32))
+    R = O.Restatement.from_csr(n, off, col)
+    np.testing.assert_array_equal(G.cc(g)[0], R.cc()[0])
+
+
+def test_saved_partitions_errors():
+    with tempfile.TemporaryDirectory() as td:
+        p = write_parts(td, 4, [[[0, 1]], [[1, 9]]])  # vertex 9 >= n
+        with pytest.raises(G.GreError) as e:
+            G.Graph.load_parts(p, 2)
+        assert e.value.status == G.GRE_INVALID_ARG
+        with pytest.raises(G.GreError) as e:
+            G.Graph.load_parts(p, 3)  # p.part.3.* missing
+        assert e.value.status == G.GRE_IO_ERROR
+        open(p + ".part.2.1", "ab").write(b"\x00" * 8)  # not whole pairs
+        with pytest.raises(G.GreError) as e:
+            G.Graph.load_parts(p, 2)
+        assert e.value.status == G.GRE_IO_ERROR
+        with pytest.raises(G.GreError) as e:
+            G.Graph.load_parts(p, 0)
+        assert e.value.status == G.GRE_INVALID_ARG
