@@ -16,7 +16,9 @@ device-resident outputs; `e2e` runs the same calls with pinned host outputs, the
 copies inside the timed region.  After the timed steps, `batched_vs_plain` reports the batched
 forms against their looped plain forms at equal results (256-source BC, 64-source BFS, 128
 personalised PageRank vectors, a batch of 32 uneven graphs; scale 20) and the PageRank adjoint
-against its forward, plus one 64-source BC batch on the scale-26 graph.
+against its forward, plus one 64-source BC batch on the scale-26 graph.  `partitioned` times the
+1D-partitioned BFS and PageRank (gre_part_*, graphine_b200/partition.py) over the ranks, NCCL
+exchanges; at one GPU a one-rank group, checked equal to the one-GPU calls.
 
 --impl reference runs the reference GRE engine (compiled from its headers into oracle/_ref/)
 on the host CPU over a bounded sample (RMAT scale 16, same plain suite) and prints the same line.
@@ -64,7 +66,8 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.lines = []
+        self.lines = []  # (arrival time, line)
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
@@ -79,7 +82,15 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
+
+    # the sampler starts before the warm-up (nvidia-smi needs a moment to print its first line);
+    # the summary keeps the samples that arrived between these marks
+    def mark_start(self):
+        self.t0 = time.perf_counter()
+
+    def mark_end(self):
+        self.t1 = time.perf_counter()
 
     def __exit__(self, *a):
         if self.proc:
@@ -92,7 +103,12 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        window = "timed"
+        lines = [ln for t, ln in self.lines
+                 if (self.t0 is None or t >= self.t0) and (self.t1 is None or t <= self.t1 + 0.1)]
+        if not lines:  # timed region shorter than the sampling period: warm-up and timed steps
+            window, lines = "warmup+timed", [ln for _, ln in self.lines]
+        for line in lines:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -105,7 +121,7 @@ class ClockSampler:
                 if parts[5 + i].lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "window": window}
 
 
 def measured_peak():
@@ -270,6 +286,61 @@ def batched_block(G, dev_index: int, scale: int, seed: int):
     return out
 
 
+def partitioned_block(G, g, srcs, world: int, rank: int, local_rank: int) -> dict:
+    """The 1D-partitioned BFS and PageRank (gre_part_*): this rank's part of the graph, the
+    exchanges through the library's own NCCL communicator on the part's stream (over the ranks of
+    the default process group; one rank when there is none, where every exchange is a local
+    copy).  Device-resident outputs; device time of each call, max over ranks.  At one rank the
+    results are compared with the one-GPU calls on the same inputs."""
+    import torch
+    import torch.distributed as tdist
+
+    from graphine_b200 import partition as PT
+
+    x = PT.NcclExchange()
+    try:
+        t0 = time.perf_counter()
+        part = PT.Part(g, world, rank)
+        build_s = time.perf_counter() - t0
+        dev = torch.device("cuda", local_rank)
+        lv = torch.empty(g.n, dtype=torch.int32, device=dev)
+        pr = torch.empty(g.n, dtype=torch.float64, device=dev)
+        part.bfs(int(srcs[0]), x, out=lv)  # warm-up (workspace allocation)
+        part.pagerank(x, G.PR_ITER, 0.85, 2, out=pr)
+        bfs_ms, edges, same_bfs = 0.0, 0, True
+        for s in srcs:
+            _, st = part.bfs(int(s), x, out=lv)
+            bfs_ms += st.device_ms
+            edges += st.traversed_edges
+            if world == 1:
+                one = torch.empty_like(lv)
+                G.bfs(g, [int(s)], out=one)
+                same_bfs = same_bfs and bool(torch.equal(one, lv))
+        _, st = part.pagerank(x, G.PR_ITER, 0.85, PR_ITERS, out=pr)
+        pr_ms, pr_bytes = st.device_ms, st.algo_bytes
+        same_pr = None
+        if world == 1:
+            one = torch.empty_like(pr)
+            G.pagerank(g, G.PR_ITER, 0.85, PR_ITERS, out=one)
+            same_pr = bool(torch.equal(one, pr))
+        if world > 1:
+            t = torch.tensor([bfs_ms, pr_ms], dtype=torch.float64, device=dev)
+            tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+            bfs_ms, pr_ms = float(t[0]), float(t[1])
+        info = {"ranks": world, "slots_per_rank": part.slots, "arcs_in_rank0": part.arcs_in, "build_s": build_s,
+                "exchange": "library NCCL communicator: all-gather / grouped send-recv on the part's stream",
+                "bfs": {"sources": len(srcs), "ms_per_source": bfs_ms / len(srcs),
+                        "gteps": edges / (bfs_ms * 1e-3) / 1e9 if bfs_ms else None},
+                "pagerank": {"iters": PR_ITERS, "ms_per_iter": pr_ms / PR_ITERS,
+                             "hbm_gbs_algorithmic": pr_bytes / (pr_ms * 1e-3) / 1e9 if pr_ms else None}}
+        if world == 1:
+            info["identical_to_one_gpu"] = {"bfs": same_bfs, "pagerank": same_pr}
+        part.free()
+        return info
+    finally:
+        x.free()
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import graphine_b200.gre as G
@@ -306,15 +377,16 @@ def run_ours(args, rank, world, local_rank):
 
     dev_outs = (pr_d, lv_d, ds_d, cc_d)
     sched = dict(zip(("lane_arcs", "cta_min", "hub_chunk", "seg_window"), g.row_schedule(True)))  # tuned on first use
-    for i in range(args.warmup):
-        suite(i, dev_outs)
-    torch.cuda.synchronize()
-    if dist:
-        tdist.barrier()
-    torch.cuda.synchronize()
-    l0 = G.launch_count()
     per = {k: {"ms": 0.0, "edges": 0, "bytes": 0, "arcs": 0} for k in names}
     with ClockSampler(local_rank) as clk:
+        for i in range(args.warmup):
+            suite(i, dev_outs)
+        torch.cuda.synchronize()
+        if dist:
+            tdist.barrier()
+        torch.cuda.synchronize()
+        l0 = G.launch_count()
+        clk.mark_start()
         for i in range(args.warmup, nsteps):
             for k, s in zip(names, suite(i, dev_outs)):
                 per[k]["ms"] += s.device_ms
@@ -322,7 +394,8 @@ def run_ours(args, rank, world, local_rank):
                 per[k]["bytes"] += s.algo_bytes
                 per[k]["arcs"] += s.arcs_traversed
         torch.cuda.synchronize()
-    launches = G.launch_count() - l0
+        clk.mark_end()
+        launches = G.launch_count() - l0
     if dist:
         tdist.barrier()
     torch.cuda.synchronize()
@@ -370,6 +443,11 @@ def run_ours(args, rank, world, local_rank):
                       "hbm_gbs_algorithmic": v["bytes"] / (v["ms"] * 1e-3) / 1e9 if v["ms"] else None,
                       "share": v["ms"] / tot_ms}
     extra = {}
+    if world == 1 or args.partitioned:
+        psrcs = np.random.default_rng(4242).choice(nz, size=4, replace=False).astype(np.uint32)  # same on all ranks
+        part_info = partitioned_block(G, g, psrcs, world, rank, local_rank)
+    else:
+        part_info = None
     if not args.no_batched:
         # sampled betweenness on the scale-26 graph in batches of 64 sources (one batch by
         # default, --bc-sources 1024 for the full sample), then the batched-vs-looped block
@@ -404,6 +482,7 @@ def run_ours(args, rank, world, local_rank):
                      "peak_kind": peak_kind, "bytes_per_launch": pr_bytes_iter,
                      "traffic": profiled_traffic() if args.scale == 26 and not args.no_reorder else None},
         "batched_vs_plain": extra,
+        "partitioned": part_info,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": 4, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
@@ -426,6 +505,8 @@ def main():
     ap.add_argument("--no-reorder", action="store_true", help="keep the generated vertex order")
     ap.add_argument("--only", default="", help="comma-separated subset of the suite (profiling runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--partitioned", action="store_true",
+                    help="also run the 1D-partitioned BFS/PageRank over the ranks (always at one GPU)")
     args = ap.parse_args()
     rank, world, local_rank = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
     if args.impl == "reference":

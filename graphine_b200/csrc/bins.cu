@@ -206,6 +206,7 @@ int build_segments(gre_graph g, DegreeBins& B, const uint64_t* off, const uint32
   return GRE_SUCCESS;
 }
 
+}  // namespace
 
 // Groups the rows of `off` by bin under `sched` (replacing what B held).
 int build_bins(gre_graph g, DegreeBins& B, const uint64_t* off, const uint32_t* col, const RowSchedule& sched) {
@@ -288,6 +289,8 @@ int build_bins(gre_graph g, DegreeBins& B, const uint64_t* off, const uint32_t* 
   B.ready = true;
   return GRE_SUCCESS;
 }
+
+namespace {
 
 int degree_key(gre_graph g, const uint64_t* off, std::string* key) {
   unsigned long long* dh = nullptr;

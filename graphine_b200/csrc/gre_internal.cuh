@@ -326,6 +326,8 @@ inline void stats_record(gre_stats* st, uint64_t active) {
 
 // Degree bins of the CSC (in = true) or CSR; built once per graph.
 int ensure_bins(gre_graph g, bool in);
+// Degree bins of the rows of `off` (g->n rows) under a fixed schedule (replacing what B held).
+int build_bins(gre_graph g, DegreeBins& B, const uint64_t* off, const uint32_t* col, const RowSchedule& sched);
 void free_bins(DegreeBins& B);
 // CSC slot -> CSR arc map; built once per graph.
 int ensure_rarc(gre_graph g);

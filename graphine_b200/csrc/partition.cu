@@ -1,0 +1,586 @@
+// 1D-partitioned single-source paths: one graph split by vertex over P ranks, one GPU each.
+//
+// The reference at np > 1 gives every vertex one master rank (GraphIngress.hpp:1126-1450) and
+// runs a superstep as: sync scatters (masters send their scatter values to the ranks that read
+// them, Engine.hpp:273-315), local compute, sync combiners (combined messages return to the
+// masters, Engine.hpp:333-374), apply.  Here rank p owns a fixed set of vertex slots together
+// with the in-arcs and out-arcs of those vertices (columns global), so a superstep is:
+//   * PageRank (pull): scatter-sync = all-gather of the owners' contributions (8 bytes per
+//     slot); compute = the degree-binned row reduction of the owned rows (rows.cuh, the same
+//     schedule as the whole graph, so every row's sum has the same association order as on one
+//     GPU); no combiner-sync.
+//   * BFS, bottom-up level: all-gather of the owners' frontier bits (one bit per slot); every
+//     owned unvisited vertex looks for a parent among its in-arcs (bfs.cu's k_bu_step on the
+//     local rows).
+//   * BFS, top-down level: each rank expands its own frontier along out-arcs into a candidate
+//     bitmap over all slots; combiner-sync = all-to-all of the bitmap's per-owner blocks; the
+//     owner ORs the P blocks it receives and claims the unvisited vertices.
+// The collectives come from the caller (gre_exchange_fn): NCCL through torch.distributed in
+// graphine_b200/partition.py, or ncclAllGather / ncclAlltoAll from C++.  Direction rule, levels
+// and PageRank values are those of the one-GPU paths.
+//
+// Vertex layout.  Internal ids are dealt to ranks one by one in snake order: round r = v / P
+// gives ranks 0, 1, .., P-1 on even rounds and P-1, .., 1, 0 on odd ones, and vertex v becomes
+// slot r of its rank.  On a degree-ordered (relabelled) graph every rank then holds the same
+// mix of hubs and leaves, in decreasing degree.  Each rank has L = 64 * ceil(ceil(n / P) / 64)
+// slots (whole bitmap words) and the exchange index of slot i of rank p is p * L + i, so every
+// per-vertex exchange is a rank-major array of P * L entries built by a plain all-gather of
+// equal blocks.  Slots past the last vertex are padding (no arcs, marked visited, never written
+// out).
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <vector>
+
+#include "gre_internal.cuh"
+#include "rows.cuh"
+
+struct gre_part_s {
+  gre_graph sub = nullptr;   // the owned rows; columns are exchange indices
+  uint64_t n = 0, m = 0;     // vertices and arcs of the whole graph
+  uint32_t nparts = 1, rank = 0;
+  uint64_t L = 0;            // vertex slots per rank (multiple of 64)
+  uint64_t arcs_in = 0, arcs_out = 0;  // arcs of the owned rows
+  uint32_t* xof = nullptr;   // caller id -> exchange index (n)
+  uint32_t* xmap = nullptr;  // exchange index -> caller id, 0xffffffff for padding (P * L)
+};
+
+namespace gre {
+
+struct BfsCounters {
+  unsigned long long next_count;
+  unsigned long long next_arcs;
+  unsigned long long scanned;
+  unsigned long long pad;
+};
+
+// kernels defined in bfs.cu
+__global__ void k_frontier_degrees(const uint32_t* __restrict__ queue, uint64_t nq, const uint64_t* __restrict__ off,
+                                   uint64_t* __restrict__ deg);
+__global__ void k_queue_to_bits(const uint32_t* __restrict__ queue, uint64_t nq, uint32_t* __restrict__ bits);
+__global__ void __launch_bounds__(256) k_bu_step(uint64_t n, const uint64_t* __restrict__ roff, const uint32_t* __restrict__ rcol,
+                                                 const uint64_t* __restrict__ off, const uint32_t* __restrict__ front,
+                                                 uint32_t* __restrict__ next, uint32_t* __restrict__ vis, int32_t* __restrict__ level,
+                                                 int32_t next_level, BfsCounters* __restrict__ c);
+__global__ void k_bits_to_queue(uint64_t n, const uint32_t* __restrict__ bits, uint32_t* __restrict__ queue,
+                                unsigned long long* __restrict__ count);
+
+namespace {
+
+template <class T>
+int ws_array(gre_graph g, int slot, uint64_t count, T** p) {
+  void* v = nullptr;
+  GRE_CHECK(g->ws.get(slot, sizeof(T) * (count ? count : 1), &v));
+  *p = (T*)v;
+  return GRE_SUCCESS;
+}
+
+// Exchange index of internal vertex v.
+__host__ __device__ __forceinline__ uint64_t part_index(uint64_t v, uint64_t P, uint64_t L) {
+  const uint64_t r = v / P, t = v - r * P;
+  const uint64_t p = (r & 1) ? P - 1 - t : t;
+  return p * L + r;
+}
+
+// Internal vertex of slot i of rank p (>= n: padding).
+__host__ __device__ __forceinline__ uint64_t part_vertex(uint64_t i, uint64_t p, uint64_t P) {
+  return i * P + ((i & 1) ? P - 1 - p : p);
+}
+
+__host__ __device__ __forceinline__ uint64_t part_slots(uint64_t n, uint64_t P) {
+  const uint64_t per = (n + P - 1) / P;
+  return 64 * (per ? (per + 63) / 64 : 1);
+}
+
+__global__ void k_part_maps(uint64_t n, uint64_t P, uint64_t L, const uint32_t* __restrict__ perm, uint32_t* __restrict__ xof,
+                            uint32_t* __restrict__ xmap) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t c = perm ? perm[v] : (uint32_t)v;
+    const uint32_t x = (uint32_t)part_index(v, P, L);
+    xof[c] = x;
+    xmap[x] = c;
+  }
+}
+
+// deg[i] = arcs of slot i (L + 1 entries, the last 0, for the exclusive scan); deg32 optional
+__global__ void k_part_degrees(uint64_t L, uint64_t p, uint64_t P, uint64_t n, const uint64_t* __restrict__ off,
+                               uint64_t* __restrict__ deg, uint32_t* __restrict__ deg32) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i <= L; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t v = i < L ? part_vertex(i, p, P) : n;
+    const uint64_t d = v < n ? off[v + 1] - off[v] : 0;
+    deg[i] = d;
+    if (deg32 && i < L) deg32[i] = (uint32_t)d;
+  }
+}
+
+// Arcs of every slot copied in stored order, columns turned into exchange indices; warp per row.
+__global__ void __launch_bounds__(256) k_part_rows(uint64_t L, uint64_t p, uint64_t P, uint64_t n, const uint64_t* __restrict__ off,
+                                                   const uint32_t* __restrict__ col, const uint64_t* __restrict__ loff,
+                                                   uint32_t* __restrict__ lcol) {
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31u;
+  for (uint64_t i = warp; i < L; i += nwarps) {
+    const uint64_t v = part_vertex(i, p, P);
+    if (v >= n) continue;
+    const uint64_t a0 = off[v], len = off[v + 1] - a0, dst = loff[i];
+    for (uint64_t k = lane; k < len; k += 32) lcol[dst + k] = (uint32_t)part_index(__ldg(col + a0 + k), P, L);
+  }
+}
+
+// padding slots (internal id >= n) start visited
+__global__ void k_part_pad_visited(uint64_t L, uint64_t p, uint64_t P, uint64_t n, uint32_t* __restrict__ vis) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < L; i += (uint64_t)gridDim.x * blockDim.x)
+    if (part_vertex(i, p, P) >= n) atomicOr(vis + (i >> 5), 1u << (i & 31u));
+}
+
+__global__ void k_part_seed(uint64_t slot, int32_t* __restrict__ level, uint32_t* __restrict__ vis, uint32_t* __restrict__ queue,
+                            const uint32_t* __restrict__ outdeg, BfsCounters* __restrict__ c) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  level[slot] = 0;
+  vis[slot >> 5] |= 1u << (slot & 31u);
+  queue[0] = (uint32_t)slot;
+  c->next_count = 1;
+  c->next_arcs = outdeg[slot];
+}
+
+// Top-down: one thread per arc of the local frontier (prefix = exclusive scan of its degrees);
+// the target's bit is set in the candidate bitmap over all P * L slots.
+__global__ void __launch_bounds__(256) k_part_expand(const uint32_t* __restrict__ queue, uint64_t nq, const uint64_t* __restrict__ prefix,
+                                                     uint64_t total, const uint64_t* __restrict__ off, const uint32_t* __restrict__ col,
+                                                     uint32_t* __restrict__ cand) {
+  for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t lo = 0, hi = nq;
+    while (hi - lo > 1) {
+      const uint64_t mid = (lo + hi) >> 1;
+      if (prefix[mid] <= t) lo = mid;
+      else hi = mid;
+    }
+    const uint32_t u = queue[lo];
+    const uint32_t x = __ldg(col + off[u] + (t - prefix[lo]));
+    const uint32_t bit = 1u << (x & 31u);
+    if (!(cand[x >> 5] & bit)) atomicOr(cand + (x >> 5), bit);
+  }
+}
+
+// Top-down claim on the owner: OR of the P received blocks (W words each), minus the visited
+// bits; claimed slots get the level and go to the next queue (in slot order within a warp).
+__global__ void k_part_claim(uint64_t W, uint64_t P, const uint32_t* __restrict__ recv, uint32_t* __restrict__ vis,
+                             int32_t* __restrict__ level, int32_t next_level, const uint32_t* __restrict__ outdeg,
+                             uint32_t* __restrict__ queue, BfsCounters* __restrict__ c) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+  unsigned long long arcs = 0;
+  for (uint64_t base = tid - lane; base < W; base += nthreads) {
+    const uint64_t w = base + lane;
+    uint32_t word = 0;
+    if (w < W) {
+      for (uint64_t q = 0; q < P; ++q) word |= recv[q * W + w];
+      const uint32_t old = vis[w];
+      word &= ~old;
+      if (word) vis[w] = old | word;
+    }
+    const uint32_t cnt = __popc(word);
+    uint32_t incl = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= (uint32_t)o) incl += t;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    unsigned long long pos = 0;
+    if (lane == 31 && total) pos = atomicAdd(&c->next_count, (unsigned long long)total);
+    pos = __shfl_sync(0xffffffffu, pos, 31) + incl - cnt;
+    uint32_t x = word;
+    while (x) {
+      const uint32_t b = __ffs(x) - 1;
+      x &= x - 1;
+      const uint32_t i = (uint32_t)(w << 5) + b;
+      level[i] = next_level;
+      arcs += outdeg[i];
+      queue[pos++] = i;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) arcs += __shfl_xor_sync(0xffffffffu, arcs, o);
+  if (lane == 0 && arcs) atomicAdd(&c->next_arcs, arcs);
+}
+
+// sum of the out-degrees of reached slots (edges with a reached endpoint)
+__global__ void k_part_reached(uint64_t L, const int32_t* __restrict__ level, const uint32_t* __restrict__ deg,
+                               unsigned long long* __restrict__ out) {
+  unsigned long long s = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < L; i += (uint64_t)gridDim.x * blockDim.x)
+    if (level[i] >= 0) s += deg[i];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31u) == 0 && s) atomicAdd(out, s);
+}
+
+// gathered rank-major values -> caller order
+template <class T>
+__global__ void k_part_out(uint64_t total, const uint32_t* __restrict__ xmap, const T* __restrict__ in, T* __restrict__ out) {
+  for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < total; x += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t c = xmap[x];
+    if (c != 0xffffffffu) out[c] = in[x];
+  }
+}
+
+struct PartGather {
+  const uint32_t* __restrict__ col;
+  const double* __restrict__ contrib;  // all P * L slots
+  __device__ __forceinline__ double operator()(uint32_t, uint64_t a) const { return __ldg(contrib + __ldg(col + a)); }
+};
+
+// pr = tele + d * sum; the power iteration refreshes the owner's contribution pr / outdeg
+struct PartFinish {
+  double* __restrict__ pr;
+  double* __restrict__ contrib;  // null: never refreshed (reference variant)
+  const uint32_t* __restrict__ outdeg;
+  double tele, d;
+  __device__ __forceinline__ void operator()(uint32_t v, double sum) const {
+    const double x = tele + d * sum;
+    pr[v] = x;
+    if (contrib) {
+      const uint32_t od = outdeg[v];
+      contrib[v] = od ? x / (double)od : 0.0;
+    }
+  }
+};
+
+__global__ void k_part_pr_init(uint64_t L, const uint32_t* __restrict__ outdeg, double tele, double* __restrict__ pr,
+                               double* __restrict__ contrib) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < L; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t od = outdeg[i];
+    pr[i] = tele;
+    contrib[i] = od ? tele / (double)od : 0.0;
+  }
+}
+
+// Rows of slots [0, L) of rank p from (off, col): *loff (L + 1) and *lcol allocated here.
+int part_rows(gre_graph s, uint64_t p, uint64_t P, uint64_t n, const uint64_t* off, const uint32_t* col, uint64_t** loff,
+              uint32_t** lcol, uint32_t** deg32, uint64_t* arcs) {
+  const uint64_t L = s->n;
+  uint64_t* deg = nullptr;
+  GRE_CHECK(ws_array(s, WS_A, L + 1, &deg));
+  GRE_CUDA(cudaMalloc(loff, sizeof(uint64_t) * (L + 1)));
+  GRE_CUDA(cudaMalloc(deg32, sizeof(uint32_t) * L));
+  k_part_degrees<<<grid_for(L + 1, 256), 256, 0, s->stream>>>(L, p, P, n, off, deg, *deg32);
+  size_t tb = 0;
+  void* tmp = nullptr;
+  cub::DeviceScan::ExclusiveSum(nullptr, tb, deg, *loff, L + 1, s->stream);
+  GRE_CHECK(s->ws.get(WS_CUB, tb, &tmp));
+  GRE_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, deg, *loff, L + 1, s->stream));
+  GRE_CUDA(cudaMemcpyAsync(arcs, *loff + L, sizeof(uint64_t), cudaMemcpyDeviceToHost, s->stream));
+  GRE_CUDA(cudaStreamSynchronize(s->stream));
+  GRE_CUDA(cudaMalloc(lcol, sizeof(uint32_t) * (*arcs ? *arcs : 1)));
+  k_part_rows<<<grid_for(L * 32, 256, 8), 256, 0, s->stream>>>(L, p, P, n, off, col, *loff, *lcol);
+  GRE_LAUNCH_CHECK();
+  return GRE_SUCCESS;
+}
+
+// One collective through the caller's exchange; a failure there becomes GRE_FAILURE.
+int exchange(gre_part p, gre_exchange_fn xchg, void* ctx, int kind, const void* send, void* recv, uint64_t bytes) {
+  const int r = xchg(ctx, kind, send, recv, bytes, (void*)p->sub->stream);
+  if (r) {
+    set_error("gre_part: the exchange callback returned %d (kind %d, %llu bytes per rank)", r, kind, (unsigned long long)bytes);
+    return GRE_FAILURE;
+  }
+  return GRE_SUCCESS;
+}
+
+// Counters of all ranks: local values in, sums (and this rank's entry) out.
+int exchange_counters(gre_part p, gre_exchange_fn xchg, void* ctx, BfsCounters* c, BfsCounters* all, BfsCounters* sum,
+                      BfsCounters* mine) {
+  GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLGATHER, c, all, sizeof(BfsCounters)));
+  std::vector<BfsCounters> h(p->nparts);
+  GRE_CUDA(cudaMemcpyAsync(h.data(), all, sizeof(BfsCounters) * p->nparts, cudaMemcpyDeviceToHost, p->sub->stream));
+  GRE_CUDA(cudaStreamSynchronize(p->sub->stream));
+  *sum = BfsCounters{0, 0, 0, 0};
+  for (const BfsCounters& x : h) {
+    sum->next_count += x.next_count;
+    sum->next_arcs += x.next_arcs;
+    sum->scanned += x.scanned;
+  }
+  if (mine) *mine = h[p->rank];
+  return GRE_SUCCESS;
+}
+
+void destroy_part(gre_part p) {
+  if (!p) return;
+  if (p->sub) {
+    cudaSetDevice(p->sub->device);
+    cudaFree(p->xof);
+    cudaFree(p->xmap);
+    destroy_graph(p->sub);
+  }
+  delete p;
+}
+
+}  // namespace
+}  // namespace gre
+
+using namespace gre;
+
+extern "C" {
+
+int gre_part_create(gre_graph g, uint32_t nparts, uint32_t rank, gre_part* out) {
+  if (!g || !out) return GRE_NULL;
+  *out = nullptr;
+  if (nparts == 0 || rank >= nparts) {
+    set_error("gre_part_create: rank %u of %u parts", rank, nparts);
+    return GRE_INVALID_ARG;
+  }
+  GRE_CHECK(use_graph(g));
+  GRE_CUDA(cudaStreamSynchronize(g->stream));  // the part's stream reads g's arrays
+  const uint64_t n = g->n, P = nparts;
+  const uint64_t L = part_slots(n, P);
+  if (P * L > 0xffffffffull) {
+    set_error("gre_part_create: %llu slots exceed 32-bit vertex ids", (unsigned long long)(P * L));
+    return GRE_INVALID_ARG;
+  }
+  // the whole graph's schedule, without source windows (those split rows by column)
+  GRE_CHECK(ensure_bins(g, true));
+  RowSchedule sched = g->bins_in.sched;
+  sched.seg_window = 0;
+  gre_part p = new gre_part_s;
+  p->n = n;
+  p->m = g->m;
+  p->nparts = nparts;
+  p->rank = rank;
+  p->L = L;
+  int st = new_graph(g->device, g->flags & ~(uint32_t)GRE_GRAPH_REORDER, &p->sub);
+  if (st) {
+    delete p;
+    return st;
+  }
+  auto build = [&]() -> int {
+    gre_graph s = p->sub;
+    s->n = L;
+    GRE_CHECK(part_rows(s, rank, P, n, g->roff, g->rcol, &s->roff, &s->rcol, &s->indeg, &p->arcs_in));
+    if (g->symmetric()) {
+      s->off = s->roff;
+      s->col = s->rcol;
+      s->outdeg = s->indeg;
+      p->arcs_out = p->arcs_in;
+    } else {
+      GRE_CHECK(part_rows(s, rank, P, n, g->off, g->col, &s->off, &s->col, &s->outdeg, &p->arcs_out));
+    }
+    s->m = p->arcs_out;
+    GRE_CUDA(cudaMalloc(&p->xof, sizeof(uint32_t) * (n ? n : 1)));
+    GRE_CUDA(cudaMalloc(&p->xmap, sizeof(uint32_t) * P * L));
+    GRE_CUDA(cudaMemsetAsync(p->xmap, 0xff, sizeof(uint32_t) * P * L, s->stream));
+    if (n) k_part_maps<<<grid_for(n, 256), 256, 0, s->stream>>>(n, P, L, g->perm, p->xof, p->xmap);
+    GRE_LAUNCH_CHECK();
+    // the row kernels read the CSC rows (build_bins works on s->n = L rows)
+    GRE_CHECK(build_bins(s, s->bins_in, s->roff, s->rcol, sched));
+    GRE_CUDA(cudaStreamSynchronize(s->stream));
+    return GRE_SUCCESS;
+  };
+  st = build();
+  if (st) {
+    destroy_part(p);
+    return st;
+  }
+  *out = p;
+  return GRE_SUCCESS;
+}
+
+int gre_part_layout(uint64_t n, uint32_t nparts, uint64_t* slots, uint32_t* index) {
+  if (!slots) return GRE_NULL;
+  if (nparts == 0) return GRE_INVALID_ARG;
+  const uint64_t P = nparts, L = part_slots(n, P);
+  if (P * L > 0xffffffffull) return GRE_INVALID_ARG;
+  *slots = L;
+  if (index)
+    for (uint64_t v = 0; v < n; ++v) index[v] = (uint32_t)part_index(v, P, L);
+  return GRE_SUCCESS;
+}
+
+int gre_part_free(gre_part p) {
+  destroy_part(p);
+  return GRE_SUCCESS;
+}
+
+int gre_part_info(gre_part p, uint64_t* slots, uint64_t* arcs_in, uint64_t* arcs_out) {
+  if (!p) return GRE_NULL;
+  if (slots) *slots = p->L;
+  if (arcs_in) *arcs_in = p->arcs_in;
+  if (arcs_out) *arcs_out = p->arcs_out;
+  return GRE_SUCCESS;
+}
+
+int gre_part_bfs(gre_part p, uint32_t src, int32_t* level, gre_exchange_fn xchg, void* ctx, gre_stats* st) {
+  if (!p || !level || !xchg) return GRE_NULL;
+  gre_graph s = p->sub;
+  GRE_CHECK(use_graph(s));
+  stats_reset(st);
+  const uint64_t n = p->n, P = p->nparts, L = p->L, W = L / 32, me = p->rank;
+  if (src >= n) {
+    set_error("gre_part_bfs: source %u out of range (n = %llu)", src, (unsigned long long)n);
+    return GRE_INVALID_ARG;
+  }
+  int32_t *lvl, *lvl_all, *dout;
+  uint32_t *vis, *queue, *nqueue, *front, *next, *front_all, *cand, *recv;
+  uint64_t *deg, *prefix;
+  BfsCounters *c, *call;
+  GRE_CHECK(ws_array(s, WS_A, L, &lvl));
+  GRE_CHECK(ws_array(s, WS_B, P * L, &lvl_all));
+  GRE_CHECK(ws_array(s, WS_C, W, &vis));
+  GRE_CHECK(ws_array(s, WS_D, L, &queue));
+  GRE_CHECK(ws_array(s, WS_E, L, &nqueue));
+  GRE_CHECK(ws_array(s, WS_F, W, &front));
+  GRE_CHECK(ws_array(s, WS_G, W, &next));
+  GRE_CHECK(ws_array(s, WS_H, P * W, &front_all));
+  GRE_CHECK(ws_array(s, WS_I, P * W, &cand));
+  GRE_CHECK(ws_array(s, WS_J, P * W, &recv));
+  GRE_CHECK(ws_array(s, WS_K, L + 1, &deg));
+  GRE_CHECK(ws_array(s, WS_L, L + 1, &prefix));
+  GRE_CHECK(ws_array(s, WS_COUNTERS, 1, &c));
+  GRE_CHECK(ws_array(s, WS_OUTBUF2, P, &call));
+  GRE_CHECK(prepare_output(s, level, n, WS_OUTBUF, &dout));
+  void* cubtmp = nullptr;
+  size_t cubbytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, cubbytes, deg, prefix, L + 1, s->stream);
+  GRE_CHECK(s->ws.get(WS_CUB, cubbytes, &cubtmp));
+
+  RunTimer timer(s);
+  uint32_t xr = 0;
+  GRE_CUDA(cudaMemcpyAsync(&xr, p->xof + src, sizeof xr, cudaMemcpyDeviceToHost, s->stream));
+  GRE_CUDA(cudaMemsetAsync(lvl, 0xff, sizeof(int32_t) * L, s->stream));
+  GRE_CUDA(cudaMemsetAsync(vis, 0, sizeof(uint32_t) * W, s->stream));
+  GRE_CUDA(cudaMemsetAsync(c, 0, sizeof(BfsCounters), s->stream));
+  k_part_pad_visited<<<grid_for(L, 256), 256, 0, s->stream>>>(L, me, P, n, vis);
+  GRE_CUDA(cudaStreamSynchronize(s->stream));
+  uint64_t nq = 0;  // local queue length
+  if (xr / L == me) {
+    k_part_seed<<<1, 32, 0, s->stream>>>(xr - me * L, lvl, vis, queue, s->outdeg, c);
+    nq = 1;
+  }
+  GRE_LAUNCH_CHECK();
+  BfsCounters sum, mine;
+  GRE_CHECK(exchange_counters(p, xchg, ctx, c, call, &sum, &mine));
+  uint64_t nf = sum.next_count, mf = sum.next_arcs;
+  int64_t mu = (int64_t)p->m - (int64_t)mf;
+  bool bottom_up = false;
+  int32_t d = 0;
+  uint64_t scanned_total = 0, bytes = 0, visited = nf;
+  const int sms = num_sms();
+  while (nf > 0) {
+    // direction choice on global counts: every rank takes the same branch
+    if (!bottom_up && (double)mf > (double)mu / 15.0 && nf > 64) {
+      GRE_CUDA(cudaMemsetAsync(front, 0, sizeof(uint32_t) * W, s->stream));
+      if (nq) k_queue_to_bits<<<grid_for(nq, 256), 256, 0, s->stream>>>(queue, nq, front);
+      GRE_LAUNCH_CHECK();
+      GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLGATHER, front, front_all, 4 * W));
+      bottom_up = true;
+    } else if (bottom_up && nf < n / 18) {
+      GRE_CUDA(cudaMemsetAsync(c, 0, sizeof(BfsCounters), s->stream));
+      k_bits_to_queue<<<grid_for(W, 256), 256, 0, s->stream>>>(L, front, queue, &c->next_count);
+      GRE_LAUNCH_CHECK();
+      unsigned long long h = 0;
+      GRE_CUDA(cudaMemcpyAsync(&h, &c->next_count, sizeof h, cudaMemcpyDeviceToHost, s->stream));
+      GRE_CUDA(cudaStreamSynchronize(s->stream));
+      nq = h;
+      bottom_up = false;
+    }
+    GRE_CUDA(cudaMemsetAsync(c, 0, sizeof(BfsCounters), s->stream));
+    if (!bottom_up) {
+      GRE_CUDA(cudaMemsetAsync(cand, 0, sizeof(uint32_t) * P * W, s->stream));
+      unsigned long long total = 0;
+      if (nq) {
+        k_frontier_degrees<<<grid_for(nq, 256), 256, 0, s->stream>>>(queue, nq, s->off, deg);
+        GRE_CUDA(cub::DeviceScan::ExclusiveSum(cubtmp, cubbytes, deg, prefix, nq + 1, s->stream));
+        GRE_CUDA(cudaMemcpyAsync(&total, prefix + nq, sizeof total, cudaMemcpyDeviceToHost, s->stream));
+        GRE_CUDA(cudaStreamSynchronize(s->stream));
+        if (total) {
+          const int grid = (int)std::min<uint64_t>((total + 255) / 256, (uint64_t)sms * 16);
+          k_part_expand<<<grid, 256, 0, s->stream>>>(queue, nq, prefix, total, s->off, s->col, cand);
+        }
+        GRE_LAUNCH_CHECK();
+      }
+      GRE_CUDA(cudaMemcpyAsync(&c->scanned, &total, sizeof total, cudaMemcpyHostToDevice, s->stream));
+      GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLTOALL, cand, recv, 4 * W));
+      k_part_claim<<<grid_for(W, 256), 256, 0, s->stream>>>(W, P, recv, vis, lvl, d + 1, s->outdeg, nqueue, c);
+      GRE_LAUNCH_CHECK();
+      std::swap(queue, nqueue);
+      bytes += 16 * nq + 8 * total + 4 * P * W * 3;
+    } else {
+      k_bu_step<<<grid_for(W * 32, 256, 8), 256, 0, s->stream>>>(L, s->roff, s->rcol, s->off, front_all, next, vis, lvl, d + 1, c);
+      GRE_LAUNCH_CHECK();
+      GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLGATHER, next, front_all, 4 * W));
+      std::swap(front, next);
+    }
+    GRE_CHECK(exchange_counters(p, xchg, ctx, c, call, &sum, &mine));
+    if (bottom_up) bytes += 16 * (L - std::min<uint64_t>(L, visited / P)) + (uint64_t)(4.125 * (double)mine.scanned) + 4 * P * W;
+    nq = mine.next_count;
+    nf = sum.next_count;
+    mf = sum.next_arcs;
+    mu -= (int64_t)mf;
+    visited += nf;
+    scanned_total += sum.scanned;
+    ++d;
+    stats_record(st, nf);
+  }
+  // reached edges (all ranks), then the levels of every slot in caller order
+  GRE_CUDA(cudaMemsetAsync(c, 0, sizeof(BfsCounters), s->stream));
+  k_part_reached<<<grid_for(L, 256), 256, 0, s->stream>>>(L, lvl, s->outdeg, &c->next_arcs);
+  GRE_LAUNCH_CHECK();
+  GRE_CHECK(exchange_counters(p, xchg, ctx, c, call, &sum, nullptr));
+  GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLGATHER, lvl, lvl_all, 4 * L));
+  k_part_out<int32_t><<<grid_for(P * L, 256), 256, 0, s->stream>>>(P * L, p->xmap, lvl_all, dout);
+  GRE_LAUNCH_CHECK();
+  GRE_CHECK(finish_output(s, level, dout, n));
+  GRE_CHECK(timer.stop(st));
+  if (st) {
+    st->supersteps = (uint32_t)(d > 0 ? d - 1 : 0);
+    st->arcs_traversed = scanned_total;
+    st->traversed_edges = s->symmetric() ? sum.next_arcs / 2 : sum.next_arcs;
+    st->algo_bytes = bytes;
+  }
+  return GRE_SUCCESS;
+}
+
+int gre_part_pagerank(gre_part p, int variant, double d, uint32_t iters, double* pr, gre_exchange_fn xchg, void* ctx,
+                      gre_stats* st) {
+  if (!p || !pr || !xchg) return GRE_NULL;
+  if ((variant != GRE_PR_REFERENCE && variant != GRE_PR_ITER) || !(d >= 0.0 && d < 1.0)) return GRE_INVALID_ARG;
+  gre_graph s = p->sub;
+  GRE_CHECK(use_graph(s));
+  stats_reset(st);
+  const uint64_t n = p->n, P = p->nparts, L = p->L;
+  double *prl, *pr_all, *contrib, *contrib_all, *partial, *dout;
+  GRE_CHECK(ws_array(s, WS_A, L, &prl));
+  GRE_CHECK(ws_array(s, WS_B, P * L, &pr_all));
+  GRE_CHECK(ws_array(s, WS_C, L, &contrib));
+  GRE_CHECK(ws_array(s, WS_D, P * L, &contrib_all));
+  GRE_CHECK(ws_array(s, WS_E, s->bins_in.n_hub_chunks + 1, &partial));
+  GRE_CHECK(prepare_output(s, pr, n, WS_OUTBUF, &dout));
+  const double tele = 1.0 - d;
+  const bool refresh = variant == GRE_PR_ITER;
+  RunTimer timer(s);
+  k_part_pr_init<<<grid_for(L, 256), 256, 0, s->stream>>>(L, s->outdeg, tele, prl, contrib);
+  GRE_LAUNCH_CHECK();
+  for (uint32_t it = 0; it < iters; ++it) {
+    // scatter-sync: every rank reads the contributions of all slots (fixed in the reference
+    // variant: gathered once)
+    if (it == 0 || refresh) GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLGATHER, contrib, contrib_all, 8 * L));
+    GRE_CHECK(rows::reduce_rows(s->bins_in, s->roff, PartGather{s->rcol, contrib_all},
+                                PartFinish{prl, refresh ? contrib : nullptr, s->outdeg, tele, d}, partial, s->stream));
+  }
+  GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLGATHER, prl, pr_all, 8 * L));
+  k_part_out<double><<<grid_for(P * L, 256), 256, 0, s->stream>>>(P * L, p->xmap, pr_all, dout);
+  GRE_LAUNCH_CHECK();
+  GRE_CHECK(finish_output(s, pr, dout, n));
+  GRE_CHECK(timer.stop(st));
+  if (st) {
+    st->supersteps = iters;
+    for (uint32_t i = 0; i < iters; ++i) stats_record(st, rows::nonempty_rows(s->bins_in));
+    st->arcs_traversed = p->arcs_in * (uint64_t)iters;  // this rank's in-arcs
+    st->traversed_edges = p->m * (uint64_t)iters;
+    // this rank: offsets, columns, gathered contributions, outdeg, pr and contribution writes,
+    // plus the P * L contributions received
+    st->algo_bytes = (8 * (L + 1) + 12 * p->arcs_in + 20 * L + 8 * P * L) * (uint64_t)iters;
+  }
+  return GRE_SUCCESS;
+}
+
+}  // extern "C"

@@ -37,6 +37,9 @@ SYMMETRIC = 0x10
 REORDER = 0x20
 PR_REFERENCE, PR_ITER = 0, 1
 MAX_RECORDED = 1024
+XCHG_ALLGATHER, XCHG_ALLTOALL = 0, 1  # enum gre_exchange_kind
+# int (*gre_exchange_fn)(void* ctx, int kind, const void* send, void* recv, uint64_t bytes, void* stream)
+EXCHANGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p)
 
 
 class GreError(RuntimeError):
@@ -136,6 +139,16 @@ def lib() -> C.CDLL:
             "gre_ppr": (I32, [P, P, U32, D, U32, I32, P, S]),
             "gre_pagerank_weighted": (I32, [P, D, P, D, U32, P, S]),
             "gre_pagerank_adjoint": (I32, [P, D, P, P, D, U32, P, P, P, S]),
+            "gre_part_create": (I32, [P, U32, U32, C.POINTER(P)]),
+            "gre_part_free": (I32, [P]),
+            "gre_part_info": (I32, [P, C.POINTER(U64), C.POINTER(U64), C.POINTER(U64)]),
+            "gre_nccl_unique_id": (I32, [P]),
+            "gre_nccl_create": (I32, [P, U32, U32, I32, C.POINTER(P)]),
+            "gre_nccl_free": (I32, [P]),
+            "gre_nccl_exchange": (I32, [P, I32, P, P, U64, P]),
+            "gre_part_layout": (I32, [U64, U32, C.POINTER(U64), P]),
+            "gre_part_bfs": (I32, [P, U32, P, EXCHANGE_FN, P, S]),
+            "gre_part_pagerank": (I32, [P, I32, D, U32, P, EXCHANGE_FN, P, S]),
             "gre_rmat_host": (I32, [U32, U32, U64, I32, C.POINTER(U64), C.POINTER(U64), C.POINTER(P), C.POINTER(P)]),
             "gre_host_free": (None, [P]),
             "gre_write_edgelists": (I32, [C.c_char_p, U64, U64, P, P, U32]),

@@ -243,6 +243,53 @@ int gre_pagerank_adjoint(gre_graph g, double d, const double* r, const double* c
                          gre_stats* st);
 
 /* ---------------------------------------------------------------------------------------
+ * 1D-partitioned single-source paths: one graph split by vertex over P ranks, one GPU each.
+ * Replaces the np > 1 superstep of SynchronousEngine (sync scatters, Engine.hpp:273-315;
+ * local compute; sync combiners, Engine.hpp:333-374; apply), with the vertex placement of
+ * GraphIngress.hpp:1126-1450 replaced by a fixed one: internal ids dealt to ranks one by one in
+ * snake order, L = 64 * ceil(ceil(n / P) / 64) slots per rank.  Each rank keeps the in- and
+ * out-arcs of its own vertices.  Results equal the one-GPU calls (levels bit-exact, PageRank
+ * with the same per-row association order when the graph's schedule has no source windows).
+ * ------------------------------------------------------------------------------------- */
+typedef struct gre_part_s* gre_part;
+
+enum gre_exchange_kind {
+  GRE_XCHG_ALLGATHER = 0, /* send: `bytes`; recv[q*bytes, (q+1)*bytes) = send of rank q */
+  GRE_XCHG_ALLTOALL = 1   /* send: P blocks of `bytes`; recv block q = block `rank` of rank q */
+};
+/* The collective between the P ranks, supplied by the caller (ncclAllGather / ncclAlltoAll,
+ * or torch.distributed).  Every rank calls it the same number of times in the same order.
+ * send and recv are device memory of the part's device.  It must run after the work already
+ * enqueued on `stream` (the part's cudaStream_t) and complete before work enqueued after it
+ * returns: enqueue it on that stream, or synchronise.  Returns 0 on success; anything else
+ * ends the call with GRE_FAILURE. */
+typedef int (*gre_exchange_fn)(void* ctx, int kind, const void* send, void* recv, uint64_t bytes,
+                               void* stream);
+/* This rank's part of graph g (on g's device): rows of its slots, columns as exchange indices,
+ * row schedule of g.  g may be freed afterwards. */
+int gre_part_create(gre_graph g, uint32_t nparts, uint32_t rank, gre_part* out);
+int gre_part_free(gre_part p);
+/* Slots per rank (L) and arcs of this rank's rows. */
+int gre_part_info(gre_part p, uint64_t* slots, uint64_t* arcs_in, uint64_t* arcs_out);
+/* Direction-optimising BFS from caller vertex `src`; every rank receives all n levels. */
+int gre_part_bfs(gre_part p, uint32_t src, int32_t* level, gre_exchange_fn xchg, void* ctx,
+                 gre_stats* st);
+/* PageRank as gre_pagerank; every rank receives all n values. */
+int gre_part_pagerank(gre_part p, int variant, double d, uint32_t iters, double* pr,
+                      gre_exchange_fn xchg, void* ctx, gre_stats* st);
+
+/* The library's own exchange: NCCL on the part's stream (NCCL is loaded at the first
+ * gre_nccl_unique_id / gre_nccl_create: libnccl.so.2 already in the process, else the
+ * system's; GRE_NOT_IMPLEMENTED when there is none).  Rank 0 makes the 128-byte id, the host
+ * hands it to every rank (any channel), each rank makes its communicator on its device. */
+typedef struct gre_nccl_s* gre_nccl;
+int gre_nccl_unique_id(uint8_t id[128]);
+int gre_nccl_create(const uint8_t id[128], uint32_t nranks, uint32_t rank, int device, gre_nccl* out);
+int gre_nccl_free(gre_nccl c);
+/* A gre_exchange_fn: pass it with ctx = the gre_nccl of this rank (nranks = the parts). */
+int gre_nccl_exchange(void* ctx, int kind, const void* send, void* recv, uint64_t bytes, void* stream);
+
+/* ---------------------------------------------------------------------------------------
  * Host utilities (CPU only, no GPU needed).
  * ------------------------------------------------------------------------------------- */
 /* RMAT CSR on the host (same arcs as gre_graph_rmat).  *row_off and *col are malloc'ed;
@@ -256,6 +303,9 @@ int gre_write_edgelists(const char* prefix, uint64_t n, uint64_t m, const uint64
 /* <prefix>.roots: "count\n v1\n v2 ..." (read by Util::loadFromFile, Util/Util.hpp:140-157). */
 int gre_write_roots(const char* prefix, const uint32_t* roots, uint32_t count);
 int gre_read_roots(const char* prefix, uint32_t* roots, uint32_t capacity, uint32_t* count);
+/* Vertex layout of gre_part_create: slots per rank (L) and, when index is not NULL, the
+ * exchange index p * L + slot of every internal vertex id v < n (n entries). */
+int gre_part_layout(uint64_t n, uint32_t nparts, uint64_t* slots, uint32_t* index);
 /* The SSSP weight function of gre_graph_set_weights_hash. */
 uint32_t gre_sssp_weight(uint64_t wseed, uint32_t u, uint32_t v);
 
