@@ -10,11 +10,21 @@
 // count and the run time.  Differences: one GPU, no MPI; SSSP weights come from the seeded
 // weight function (environment GRE_WSEED, default 1) instead of unseeded rand(); BC runs all
 // roots of the file and accumulates them.  Exit status 0 on success, the gre status otherwise.
+//
+//   gre_run <part_bfs|part_pagerank|part_pagerank_iter> <prefix> --ranks P --rank r --id-file F [--device d]
+//
+// One rank of an np = P job over P GPUs (the reference's mpirun -np P): every rank loads the
+// graph, keeps its part (gre/gre.hpp PartitionedGraph) and runs over the library's NCCL
+// communicator.  Rank 0 writes the communicator id to F, the others wait for it (up to 120 s).
+// Every rank prints the same lines; rank 0's are the job's.
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 
+#include <chrono>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/gre/gre.hpp"
@@ -24,13 +34,94 @@ static void print_supersteps(const gre_stats& st) {
     printf("Superstep-%u: Number of active vertices...%llu\n", i, (unsigned long long)st.active[i]);
 }
 
+// The communicator id through a file: rank 0 writes it whole (temporary name, then rename).
+static std::vector<uint8_t> shared_id(const std::string& path, int rank) {
+  if (rank == 0) {
+    std::vector<uint8_t> id = gre::Underlying::uniqueId();
+    const std::string tmp = path + ".tmp";
+    FILE* f = fopen(tmp.c_str(), "wb");
+    if (!f || fwrite(id.data(), 1, id.size(), f) != id.size() || fclose(f) != 0 || rename(tmp.c_str(), path.c_str()))
+      throw gre::Error(GRE_IO_ERROR, "cannot write the id file " + path);
+    return id;
+  }
+  for (int i = 0; i < 12000; ++i) {  // 120 s
+    if (FILE* f = fopen(path.c_str(), "rb")) {
+      std::vector<uint8_t> id(128);
+      const size_t got = fread(id.data(), 1, id.size(), f);
+      fclose(f);
+      if (got == id.size()) return id;
+    }
+    std::this_thread::sleep_for(std::chrono::milliseconds(10));
+  }
+  throw gre::Error(GRE_TIMEOUT, "no id file " + path + " from rank 0");
+}
+
+static int run_partitioned(const std::string& algo, const std::string& prefix, int argc, char** argv) {
+  int ranks = 1, rank = 0, device = 0;
+  std::string id_file;
+  for (int i = 3; i + 1 < argc; i += 2) {
+    const std::string k(argv[i]);
+    if (k == "--ranks") ranks = atoi(argv[i + 1]);
+    else if (k == "--rank") rank = atoi(argv[i + 1]);
+    else if (k == "--device") device = atoi(argv[i + 1]);
+    else if (k == "--id-file") id_file = argv[i + 1];
+    else {
+      fprintf(stderr, "unknown option %s\n", k.c_str());
+      return 2;
+    }
+  }
+  if (ranks < 1 || rank < 0 || rank >= ranks || id_file.empty()) {
+    fprintf(stderr, "need --ranks P --rank r (0 <= r < P) --id-file F\n");
+    return 2;
+  }
+  gre::Underlying comm(shared_id(id_file, rank), ranks, rank, device);
+  gre_stats st{};
+  {
+    gre::DistributedGraph g;
+    if (algo == "part_bfs") g.ingress<gre::InOut>(prefix, "ascii", "edgelists", false, true, device);
+    else g.ingress<gre::Out>(prefix, "ascii", "edgelists", false, true, device);
+    gre::PartitionedGraph part(g, comm);
+    if (algo == "part_bfs") {
+      std::vector<uint32_t> roots(1024);
+      uint32_t nroots = 0;
+      int s = gre_read_roots(prefix.c_str(), roots.data(), (uint32_t)roots.size(), &nroots);
+      if ((s != GRE_SUCCESS && s != GRE_NOBUFFER) || nroots == 0) {
+        fprintf(stderr, "Err in reading src vertex from file.\n");
+        return s ? s : GRE_IO_ERROR;
+      }
+      std::vector<int32_t> level = part.bfs(roots[0], &st);
+      print_supersteps(st);
+      long reached = 0;
+      for (int32_t l : level) reached += l >= 0;
+      printf("Reached vertices: %ld\n", reached);
+    } else {
+      std::vector<double> pr = part.pagerank(algo == "part_pagerank_iter", 0.85, algo == "part_pagerank" ? 10 : 20, &st);
+      double sum = 0;
+      for (double x : pr) sum += x;
+      printf("Sum of pr: %.15g\n", sum);
+    }
+  }
+  printf("B200 | rank %d of %d | Iteration count: %u\n", rank, ranks, st.supersteps);
+  printf("B200 | Use time: %gs\n", st.device_ms * 1e-3);
+  return 0;
+}
+
 int main(int argc, char** argv) {
   if (argc < 3) {
-    fprintf(stderr, "usage: %s pagerank|pagerank_iter|pagerank_delta|bfs|sssp|sssp1|cc|cin|bc prefix [ascii] [edgelists]\n",
-            argv[0]);
+    fprintf(stderr, "usage: %s pagerank|pagerank_iter|pagerank_delta|bfs|sssp|sssp1|cc|cin|bc prefix [ascii] [edgelists]\n"
+                    "       %s part_bfs|part_pagerank|part_pagerank_iter prefix --ranks P --rank r --id-file F [--device d]\n",
+            argv[0], argv[0]);
     return 2;
   }
   const std::string algo(argv[1]), prefix(argv[2]);
+  if (algo.rfind("part_", 0) == 0) {
+    try {
+      return run_partitioned(algo, prefix, argc, argv);
+    } catch (const gre::Error& e) {
+      fprintf(stderr, "%s\n", e.what());
+      return e.status;
+    }
+  }
   try {
     gre::DistributedGraph g;
     const bool in_out = algo == "bfs" || algo == "cc" || algo == "bc" || algo == "cin";

@@ -8,8 +8,9 @@
 //   engine.getSuperstepCount(); engine.finalize();
 // (Graph/DistributedGraph.hpp:153-172, Graph/VertexSet.hpp:286-347, Engine/Engine.hpp:94-202).
 // This header keeps those names for the five reference plugins.  The communicator and buffer
-// pool disappear (one GPU, no MPI); errors are reported as gre::Error exceptions carrying the
+// pool disappear for one GPU; errors are reported as gre::Error exceptions carrying the
 // status code instead of exit(-1).  Results are read from the plugin objects after run().
+// An np > 1 job (one GPU per rank) uses Underlying (the communicator) and PartitionedGraph.
 #pragma once
 #include <stdint.h>
 
@@ -192,6 +193,67 @@ class SynchronousEngine {
   VC& vc_;
   uint32_t max_ = 1024;
   gre_stats st_{};
+};
+
+// COMM::Underlying (Comm/CommUnderlying.hpp:25-80) of an np > 1 job: the library's NCCL
+// communicator over the job's ranks, rank() and size() as in the reference.  Agreeing on the
+// ranks (MPI_Init's part) is the job's: rank 0 makes the id with uniqueId() and hands it to every
+// rank (a file, a launcher, a socket); each rank builds its communicator on its device.
+class Underlying {
+ public:
+  static std::vector<uint8_t> uniqueId() {
+    std::vector<uint8_t> id(128);
+    check(gre_nccl_unique_id(id.data()), "gre_nccl_unique_id");
+    return id;
+  }
+  Underlying(const std::vector<uint8_t>& id, int size, int rank, int device = 0) : size_(size), rank_(rank) {
+    if (id.size() != 128) throw Error(GRE_INVALID_ARG, "Underlying: the id has 128 bytes");
+    check(gre_nccl_create(id.data(), (uint32_t)size, (uint32_t)rank, device, &c_), "gre_nccl_create");
+  }
+  Underlying(const Underlying&) = delete;
+  Underlying& operator=(const Underlying&) = delete;
+  ~Underlying() {
+    if (c_) gre_nccl_free(c_);
+  }
+  int rank() const { return rank_; }
+  int size() const { return size_; }
+  gre_nccl handle() const { return c_; }
+
+ private:
+  gre_nccl c_ = nullptr;
+  int size_ = 1, rank_ = 0;
+};
+
+// This rank's part of a graph split by vertex over the ranks of `comm` (gre_part_create):
+// built from the graph the rank loaded, which may be released afterwards.  Every rank gets the
+// results of all vertices.
+class PartitionedGraph {
+ public:
+  PartitionedGraph(const DistributedGraph& g, Underlying& comm) : comm_(comm), n_(g.get_num_masters()) {
+    check(gre_part_create(g.handle(), (uint32_t)comm.size(), (uint32_t)comm.rank(), &p_), "gre_part_create");
+  }
+  PartitionedGraph(const PartitionedGraph&) = delete;
+  PartitionedGraph& operator=(const PartitionedGraph&) = delete;
+  ~PartitionedGraph() {
+    if (p_) gre_part_free(p_);
+  }
+  std::vector<int32_t> bfs(uint32_t src, gre_stats* st = nullptr) {
+    std::vector<int32_t> level(n_);
+    check(gre_part_bfs(p_, src, level.data(), gre_nccl_exchange, comm_.handle(), st), "gre_part_bfs");
+    return level;
+  }
+  std::vector<double> pagerank(bool iter, double d, uint32_t iters, gre_stats* st = nullptr) {
+    std::vector<double> pr(n_);
+    check(gre_part_pagerank(p_, iter ? GRE_PR_ITER : GRE_PR_REFERENCE, d, iters, pr.data(), gre_nccl_exchange,
+                            comm_.handle(), st),
+          "gre_part_pagerank");
+    return pr;
+  }
+
+ private:
+  Underlying& comm_;
+  size_t n_;
+  gre_part p_ = nullptr;
 };
 
 }  // namespace gre

@@ -52,3 +52,28 @@ def test_driver_reports_bad_input_with_status():
     with tempfile.TemporaryDirectory() as td:
         p = subprocess.run([DRIVER, "cc", os.path.join(td, "absent")], capture_output=True, text=True, timeout=60)
         assert p.returncode == G.GRE_IO_ERROR
+
+
+def test_partitioned_driver_one_rank(golden):
+    case = golden["rmat_s10_sym"]
+    n = int(case["n"])
+    with tempfile.TemporaryDirectory() as td:
+        prefix = os.path.join(td, "g")
+        G.write_edgelists(prefix, n, case["off"], case["col"], 4)
+        G.write_roots(prefix, case["roots"])
+        idf = os.path.join(td, "nccl.id")
+        args = ["--ranks", "1", "--rank", "0", "--id-file", idf]
+        p = subprocess.run([DRIVER, "part_bfs", prefix] + args, capture_output=True, text=True, timeout=300)
+        assert p.returncode == 0, p.stderr
+        counts = [int(x) for x in re.findall(r"Superstep-\d+: Number of active vertices\.\.\.(\d+)", p.stdout)]
+        g = G.Graph.ingress(prefix, dir=G.InOut)
+        lv, st = G.bfs(g, [int(case["roots"][0])])
+        assert counts == st.active
+        assert f"Reached vertices: {int((lv >= 0).sum())}" in p.stdout
+        p = subprocess.run([DRIVER, "part_pagerank_iter", prefix] + args, capture_output=True, text=True, timeout=300)
+        assert p.returncode == 0, p.stderr
+        pr, _ = G.pagerank(G.Graph.ingress(prefix, dir=G.Out), G.PR_ITER, 0.85, 20)
+        s = 0.0
+        for x in pr:  # the driver's order of summation
+            s += float(x)
+        assert f"Sum of pr: {s:.15g}" in p.stdout

@@ -7,7 +7,10 @@ back into) is checked on gloo ranks with host buffers.  The partitioned kernels 
 in test_gpu_partition.py.
 """
 import ctypes as C
+import os
 import socket
+import subprocess
+import tempfile
 
 import numpy as np
 import pytest
@@ -103,3 +106,23 @@ def test_torch_exchange_semantics_over_gloo(world):
         np.testing.assert_array_equal(gathered, np.repeat(np.arange(1, world + 1), nb))
         # block q of rank r's receive buffer = block r of rank q's send buffer
         np.testing.assert_array_equal(a2a, np.repeat(np.arange(world) + r * 16, nb))
+
+
+DRIVER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "graphine_b200", "drivers", "gre_run")
+
+
+def test_driver_partitioned_arguments_and_id_file():
+    with tempfile.TemporaryDirectory() as td:
+        prefix = os.path.join(td, "g")
+        bad = subprocess.run([DRIVER, "part_bfs", prefix, "--ranks", "2", "--rank", "2", "--id-file", "x"],
+                             capture_output=True, text=True, timeout=60)
+        assert bad.returncode == 2
+        bad = subprocess.run([DRIVER, "part_bfs", prefix, "--ranks", "1"], capture_output=True, text=True, timeout=60)
+        assert bad.returncode == 2
+        # rank 0 publishes the communicator id whole before it needs a GPU
+        idf = os.path.join(td, "nccl.id")
+        p = subprocess.run([DRIVER, "part_bfs", prefix, "--ranks", "1", "--rank", "0", "--id-file", idf],
+                           capture_output=True, text=True, timeout=120)
+        if G.device_count() == 0:
+            assert p.returncode != 0
+        assert os.path.getsize(idf) == 128 and not os.path.exists(idf + ".tmp")
