@@ -17,8 +17,8 @@ copies inside the timed region.  After the timed steps, `batched_vs_plain` repor
 forms against their looped plain forms at equal results (256-source BC, 64-source BFS, 128
 personalised PageRank vectors, a batch of 32 uneven graphs; scale 20) and the PageRank adjoint
 against its forward, plus one 64-source BC batch on the scale-26 graph.  `partitioned` times the
-1D-partitioned BFS and PageRank (gre_part_*, graphine_b200/partition.py) over the ranks, NCCL
-exchanges; at one GPU a one-rank group, checked equal to the one-GPU calls.
+1D-partitioned BFS, PageRank, SSSP and CC (gre_part_*, graphine_b200/partition.py) over the
+ranks, NCCL exchanges; at one GPU a one-rank communicator, checked equal to the one-GPU calls.
 
 --impl reference runs the reference GRE engine (compiled from its headers into oracle/_ref/)
 on the host CPU over a bounded sample (RMAT scale 16, same plain suite) and prints the same line.
@@ -287,7 +287,7 @@ def batched_block(G, dev_index: int, scale: int, seed: int):
 
 
 def partitioned_block(G, g, srcs, world: int, rank: int, local_rank: int) -> dict:
-    """The 1D-partitioned BFS and PageRank (gre_part_*): this rank's part of the graph, the
+    """The 1D-partitioned paths (gre_part_*): this rank's part of the graph, the
     exchanges through the library's own NCCL communicator on the part's stream (over the ranks of
     the default process group; one rank when there is none, where every exchange is a local
     copy).  Device-resident outputs; device time of each call, max over ranks.  At one rank the
@@ -323,18 +323,37 @@ def partitioned_block(G, g, srcs, world: int, rank: int, local_rank: int) -> dic
             one = torch.empty_like(pr)
             G.pagerank(g, G.PR_ITER, 0.85, PR_ITERS, out=one)
             same_pr = bool(torch.equal(one, pr))
+        # SSSP (frontier Bellman-Ford, one all-to-all of offers per superstep) and CC (label
+        # propagation, one all-gather per superstep) from the first source
+        ds = torch.empty(g.n, dtype=torch.int32, device=dev)
+        part.sssp(int(srcs[0]), x, out=ds)
+        _, st = part.sssp(int(srcs[0]), x, out=ds)
+        sssp_ms, sssp_edges, sssp_steps = st.device_ms, st.traversed_edges, st.supersteps
+        cc_l = torch.empty(g.n, dtype=torch.int32, device=dev)
+        _, st = part.cc(x, out=cc_l)
+        cc_ms, cc_steps = st.device_ms, st.supersteps
+        same_sssp = same_cc = None
+        if world == 1:
+            one = torch.empty_like(ds)
+            G.sssp(g, [int(srcs[0])], out=one)
+            same_sssp = bool(torch.equal(one, ds))
+            G.cc(g, out=one)
+            same_cc = bool(torch.equal(one, cc_l))
         if world > 1:
-            t = torch.tensor([bfs_ms, pr_ms], dtype=torch.float64, device=dev)
+            t = torch.tensor([bfs_ms, pr_ms, sssp_ms, cc_ms], dtype=torch.float64, device=dev)
             tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-            bfs_ms, pr_ms = float(t[0]), float(t[1])
+            bfs_ms, pr_ms, sssp_ms, cc_ms = (float(v) for v in t)
         info = {"ranks": world, "slots_per_rank": part.slots, "arcs_in_rank0": part.arcs_in, "build_s": build_s,
                 "exchange": "library NCCL communicator: all-gather / grouped send-recv on the part's stream",
                 "bfs": {"sources": len(srcs), "ms_per_source": bfs_ms / len(srcs),
                         "gteps": edges / (bfs_ms * 1e-3) / 1e9 if bfs_ms else None},
                 "pagerank": {"iters": PR_ITERS, "ms_per_iter": pr_ms / PR_ITERS,
-                             "hbm_gbs_algorithmic": pr_bytes / (pr_ms * 1e-3) / 1e9 if pr_ms else None}}
+                             "hbm_gbs_algorithmic": pr_bytes / (pr_ms * 1e-3) / 1e9 if pr_ms else None},
+                "sssp": {"ms": sssp_ms, "supersteps": sssp_steps,
+                         "gteps": sssp_edges / (sssp_ms * 1e-3) / 1e9 if sssp_ms else None},
+                "cc": {"ms": cc_ms, "supersteps": cc_steps}}
         if world == 1:
-            info["identical_to_one_gpu"] = {"bfs": same_bfs, "pagerank": same_pr}
+            info["identical_to_one_gpu"] = {"bfs": same_bfs, "pagerank": same_pr, "sssp": same_sssp, "cc": same_cc}
         part.free()
         return info
     finally:

@@ -333,6 +333,17 @@ void free_bins(DegreeBins& B);
 int ensure_rarc(gre_graph g);
 // Undirected edge count with both endpoints in a reached set (Graph500 TEPS numerator).
 int count_reached_edges(gre_graph g, const int32_t* level, uint64_t* edges, uint64_t rows = 1);
+// SSSP bucket width: half the mean uint32 weight (GRE_SSSP_DELTA overrides; 0 = no buckets).
+int sssp_delta(gre_graph g, uint32_t* delta);
+// One edge-balanced relaxation pass (sssp.cu): the frontier `queue` (nq vertices, exclusive
+// scan `prefix` of their arc counts, `total` arcs starting at base[u]) offers srcdist[u] + w to
+// dist[head] (atomic min).  srcdist == dist: the one-GPU relaxation, a `changed` bit per
+// improved head; otherwise dist is a separate offer array and changed is unused.  tstart holds
+// ceil(total / sssp_tile_arcs()) entries; error is set if a tile holds too many owners.
+uint64_t sssp_tile_arcs();
+int sssp_relax_tiles(cudaStream_t stream, const uint32_t* queue, uint64_t nq, const uint64_t* prefix, uint64_t total,
+                     uint32_t* tstart, const uint64_t* base, const uint32_t* col, const uint32_t* w, const uint32_t* srcdist,
+                     uint32_t* dist, uint32_t* changed, uint32_t* error);
 // Direction-optimising BFS levels from device roots (uses slots WS_A..WS_G, WS_COUNTERS, WS_CUB).
 int bfs_levels(gre_graph g, const uint32_t* droots, uint32_t nroots, int32_t* level, gre_stats* st, bool record);
 

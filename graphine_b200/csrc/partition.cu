@@ -41,6 +41,8 @@ struct gre_part_s {
   uint32_t nparts = 1, rank = 0;
   uint64_t L = 0;            // vertex slots per rank (multiple of 64)
   uint64_t arcs_in = 0, arcs_out = 0;  // arcs of the owned rows
+  uint32_t* w32 = nullptr;   // weights of the out-arc rows (the graph's, when it had them)
+  uint32_t delta = 0;        // SSSP bucket width: half the mean weight (0: no buckets)
   uint32_t* xof = nullptr;   // caller id -> exchange index (n)
   uint32_t* xmap = nullptr;  // exchange index -> caller id, 0xffffffff for padding (P * L)
 };
@@ -215,6 +217,16 @@ __global__ void k_part_reached(uint64_t L, const int32_t* __restrict__ level, co
   if ((threadIdx.x & 31u) == 0 && s) atomicAdd(out, s);
 }
 
+// sum of the out-degrees of slots with a finite distance
+__global__ void k_part_reached_dist(uint64_t L, const uint32_t* __restrict__ dist, const uint32_t* __restrict__ deg,
+                                    unsigned long long* __restrict__ out) {
+  unsigned long long s = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < L; i += (uint64_t)gridDim.x * blockDim.x)
+    if (dist[i] != 0xffffffffu) s += deg[i];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31u) == 0 && s) atomicAdd(out, s);
+}
+
 // gathered rank-major values -> caller order
 template <class T>
 __global__ void k_part_out(uint64_t total, const uint32_t* __restrict__ xmap, const T* __restrict__ in, T* __restrict__ out) {
@@ -253,6 +265,168 @@ __global__ void k_part_pr_init(uint64_t L, const uint32_t* __restrict__ outdeg, 
     pr[i] = tele;
     contrib[i] = od ? tele / (double)od : 0.0;
   }
+}
+
+// Arc weights of the slots' rows in stored order (the same order as k_part_rows).
+__global__ void __launch_bounds__(256) k_part_weights(uint64_t L, uint64_t p, uint64_t P, uint64_t n,
+                                                      const uint64_t* __restrict__ off, const uint32_t* __restrict__ w,
+                                                      const uint64_t* __restrict__ loff, uint32_t* __restrict__ lw) {
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31u;
+  for (uint64_t i = warp; i < L; i += nwarps) {
+    const uint64_t v = part_vertex(i, p, P);
+    if (v >= n) continue;
+    const uint64_t a0 = off[v], len = off[v + 1] - a0, dst = loff[i];
+    for (uint64_t k = lane; k < len; k += 32) lw[dst + k] = __ldg(w + a0 + k);
+  }
+}
+
+// SSSP claim on the owner: the smallest of the P offers for each slot; an improvement lowers the
+// distance and marks the slot pending (to be relaxed when its bucket comes; slots without
+// out-arcs never are).  One warp covers 32 consecutive slots, i.e. one pending word.
+__global__ void k_part_sssp_claim(uint64_t L, uint64_t P, const uint32_t* __restrict__ recv, uint32_t* __restrict__ dist,
+                                  const uint32_t* __restrict__ outdeg, uint32_t* __restrict__ pend) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) & ~31ull; base < L; base += stride) {
+    const uint64_t i = base + (threadIdx.x & 31u);
+    bool mark = false;
+    if (i < L) {
+      uint32_t m = 0xffffffffu;
+      for (uint64_t q = 0; q < P; ++q) m = min(m, recv[q * L + i]);
+      if (m < dist[i]) {
+        dist[i] = m;
+        mark = outdeg[i] != 0;
+      }
+    }
+    const uint32_t ball = __ballot_sync(0xffffffffu, mark);
+    if ((threadIdx.x & 31u) == 0 && ball) pend[base >> 5] |= ball;
+  }
+}
+
+// Near-far selection (Davidson et al., IPDPS 2014): pending slots below the limit form this
+// superstep's frontier (their pending bits are cleared); the others stay pending, and the
+// smallest of their distances is kept (to raise the limit when the near set runs dry).
+struct SsspCounters {
+  unsigned long long near;     // queued this superstep
+  unsigned long long pending;  // left pending (at or above the limit)
+  unsigned long long min_far;  // smallest distance left pending
+  unsigned long long arcs;     // out-arcs of the queued slots
+};
+
+__global__ void k_part_sssp_select(uint64_t W, uint32_t* __restrict__ pend, const uint32_t* __restrict__ dist, uint32_t limit,
+                                   const uint32_t* __restrict__ outdeg, uint32_t* __restrict__ queue,
+                                   SsspCounters* __restrict__ c) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  unsigned long long left = 0, arcs = 0;
+  uint32_t dmin = 0xffffffffu;
+  for (uint64_t base = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) & ~31ull; base < W; base += stride) {
+    const uint64_t w = base + (threadIdx.x & 31u);
+    uint32_t bits = w < W ? pend[w] : 0u, keep = 0;
+    while (__any_sync(0xffffffffu, bits != 0)) {
+      bool take = false;
+      uint32_t i = 0;
+      if (bits) {
+        const uint32_t b = __ffs(bits) - 1;
+        bits &= bits - 1;
+        i = (uint32_t)(w << 5) + b;
+        const uint32_t d = dist[i];
+        if (d < limit) {
+          take = outdeg[i] != 0;  // a source without out-arcs has nothing to offer
+          arcs += outdeg[i];
+        } else {
+          keep |= 1u << b;
+          ++left;
+          dmin = min(dmin, d);
+        }
+      }
+      const uint32_t pos = warp_append((uint32_t*)&c->near, take);
+      if (take) queue[pos] = i;
+    }
+    if (w < W && pend[w] != keep) pend[w] = keep;
+  }
+  dmin = __reduce_min_sync(0xffffffffu, dmin);
+  for (int o = 16; o > 0; o >>= 1) {
+    left += __shfl_xor_sync(0xffffffffu, left, o);
+    arcs += __shfl_xor_sync(0xffffffffu, arcs, o);
+  }
+  if ((threadIdx.x & 31u) == 0) {
+    if (left) atomicAdd(&c->pending, left);
+    if (arcs) atomicAdd(&c->arcs, arcs);
+    if (dmin != 0xffffffffu) atomicMin(&c->min_far, (unsigned long long)dmin);
+  }
+}
+
+// CC labels start as the caller ids of the slots (padding: none)
+__global__ void k_part_cc_init(uint64_t L, const uint32_t* __restrict__ xmap_rank, uint32_t* __restrict__ lab) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < L; i += (uint64_t)gridDim.x * blockDim.x)
+    lab[i] = xmap_rank[i];
+}
+
+// New label of row v from the smallest neighbour label m (UINT32_MAX: none): the shortcut
+// through the vertices the labels name, and a lower value replaces the label.
+__device__ __forceinline__ bool cc_update(uint32_t v, uint32_t m, const uint32_t* __restrict__ lab_all,
+                                          const uint32_t* __restrict__ xof, uint32_t* __restrict__ lab) {
+  const uint32_t cur = lab[v];
+  if (m != 0xffffffffu) m = min(m, lab_all[xof[m]]);
+  if (cur != 0xffffffffu) m = min(m, lab_all[xof[cur]]);
+  if (m < cur) {
+    lab[v] = m;
+    return true;
+  }
+  return false;
+}
+
+// CC, one superstep over the rows of one degree bin, G lanes per row (bins 0-5 of the row
+// schedule): the smallest label among the row's neighbours (labels of all slots from the
+// previous superstep), then cc_update.
+template <int G>
+__global__ void __launch_bounds__(256) k_part_cc_lanes(const uint32_t* __restrict__ rows, uint64_t count,
+                                                       const uint64_t* __restrict__ off, const uint32_t* __restrict__ col,
+                                                       const uint32_t* __restrict__ lab_all, const uint32_t* __restrict__ xof,
+                                                       uint32_t* __restrict__ lab, BfsCounters* __restrict__ c) {
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint32_t lig = threadIdx.x % G;
+  const uint64_t ngroups = ((uint64_t)gridDim.x * blockDim.x) / G;
+  unsigned long long changed = 0;
+  // warp-uniform trip count: every lane takes part in the shuffles
+  for (uint64_t base = (tid / G) & ~(uint64_t)(32 / G - 1); base < count; base += ngroups) {
+    const uint64_t r = base + (threadIdx.x & 31u) / G;
+    uint32_t m = 0xffffffffu, v = 0;
+    if (r < count) {
+      v = rows[r];
+      for (uint64_t a = off[v] + lig; a < off[v + 1]; a += G) m = min(m, lab_all[__ldg(col + a)]);
+    }
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (r < count && lig == 0 && cc_update(v, m, lab_all, xof, lab)) ++changed;
+  }
+  if (changed) atomicAdd(&c->next_count, changed);
+}
+
+// CC for the long rows (bins 6-7): CTA per row.
+__global__ void __launch_bounds__(256) k_part_cc_rows(const uint32_t* __restrict__ rows, uint64_t count,
+                                                      const uint64_t* __restrict__ off, const uint32_t* __restrict__ col,
+                                                      const uint32_t* __restrict__ lab_all, const uint32_t* __restrict__ xof,
+                                                      uint32_t* __restrict__ lab, BfsCounters* __restrict__ c) {
+  __shared__ uint32_t s_min[8];
+  const uint32_t lane = threadIdx.x & 31u;
+  unsigned long long changed = 0;
+  for (uint64_t r = blockIdx.x; r < count; r += gridDim.x) {
+    const uint32_t v = rows[r];
+    uint32_t m = 0xffffffffu;
+    for (uint64_t a = off[v] + threadIdx.x; a < off[v + 1]; a += blockDim.x) m = min(m, lab_all[__ldg(col + a)]);
+    m = __reduce_min_sync(0xffffffffu, m);
+    if (lane == 0) s_min[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      m = threadIdx.x < (blockDim.x >> 5) ? s_min[threadIdx.x] : 0xffffffffu;
+      m = __reduce_min_sync(0xffffffffu, m);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && cc_update(v, m, lab_all, xof, lab)) ++changed;
+  }
+  if (changed) atomicAdd(&c->next_count, changed);
 }
 
 // Rows of slots [0, L) of rank p from (off, col): *loff (L + 1) and *lcol allocated here.
@@ -310,6 +484,7 @@ void destroy_part(gre_part p) {
     cudaSetDevice(p->sub->device);
     cudaFree(p->xof);
     cudaFree(p->xmap);
+    cudaFree(p->w32);
     destroy_graph(p->sub);
   }
   delete p;
@@ -365,6 +540,12 @@ int gre_part_create(gre_graph g, uint32_t nparts, uint32_t rank, gre_part* out) 
       GRE_CHECK(part_rows(s, rank, P, n, g->off, g->col, &s->off, &s->col, &s->outdeg, &p->arcs_out));
     }
     s->m = p->arcs_out;
+    if (g->w32) {
+      GRE_CUDA(cudaMalloc(&p->w32, sizeof(uint32_t) * (p->arcs_out ? p->arcs_out : 1)));
+      k_part_weights<<<grid_for(L * 32, 256, 8), 256, 0, s->stream>>>(L, rank, P, n, g->off, g->w32, s->off, p->w32);
+      GRE_LAUNCH_CHECK();
+      GRE_CHECK(sssp_delta(g, &p->delta));  // the whole graph's, the same on every rank
+    }
     GRE_CUDA(cudaMalloc(&p->xof, sizeof(uint32_t) * (n ? n : 1)));
     GRE_CUDA(cudaMalloc(&p->xmap, sizeof(uint32_t) * P * L));
     GRE_CUDA(cudaMemsetAsync(p->xmap, 0xff, sizeof(uint32_t) * P * L, s->stream));
@@ -372,6 +553,7 @@ int gre_part_create(gre_graph g, uint32_t nparts, uint32_t rank, gre_part* out) 
     GRE_LAUNCH_CHECK();
     // the row kernels read the CSC rows (build_bins works on s->n = L rows)
     GRE_CHECK(build_bins(s, s->bins_in, s->roff, s->rcol, sched));
+    if (!g->symmetric()) GRE_CHECK(build_bins(s, s->bins_out, s->off, s->col, sched));  // CC pulls both ways
     GRE_CUDA(cudaStreamSynchronize(s->stream));
     return GRE_SUCCESS;
   };
@@ -579,6 +761,194 @@ int gre_part_pagerank(gre_part p, int variant, double d, uint32_t iters, double*
     // this rank: offsets, columns, gathered contributions, outdeg, pr and contribution writes,
     // plus the P * L contributions received
     st->algo_bytes = (8 * (L + 1) + 12 * p->arcs_in + 20 * L + 8 * P * L) * (uint64_t)iters;
+  }
+  return GRE_SUCCESS;
+}
+
+int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg, void* ctx, gre_stats* st) {
+  if (!p || !dist || !xchg) return GRE_NULL;
+  gre_graph s = p->sub;
+  GRE_CHECK(use_graph(s));
+  stats_reset(st);
+  const uint64_t n = p->n, P = p->nparts, L = p->L, W = L / 32, me = p->rank;
+  if (!p->w32) {
+    set_error("gre_part_sssp: the graph had no uint32 weights when the part was made");
+    return GRE_INVALID_ARG;
+  }
+  if (src >= n) {
+    set_error("gre_part_sssp: source %u out of range (n = %llu)", src, (unsigned long long)n);
+    return GRE_INVALID_ARG;
+  }
+  uint32_t *dl, *dist_all, *queue, *pend, *cand, *recv, *dout;
+  uint64_t *deg, *prefix;
+  SsspCounters *c, *call;
+  BfsCounters *bc, *bcall;
+  GRE_CHECK(ws_array(s, WS_A, L, &dl));
+  GRE_CHECK(ws_array(s, WS_B, P * L, &dist_all));
+  GRE_CHECK(ws_array(s, WS_C, W, &pend));
+  GRE_CHECK(ws_array(s, WS_D, L, &queue));
+  GRE_CHECK(ws_array(s, WS_I, P * L, &cand));
+  GRE_CHECK(ws_array(s, WS_J, P * L, &recv));
+  GRE_CHECK(ws_array(s, WS_K, L + 1, &deg));
+  GRE_CHECK(ws_array(s, WS_L, L + 1, &prefix));
+  uint32_t *tstart, *err;
+  GRE_CHECK(ws_array(s, WS_E, p->arcs_out / sssp_tile_arcs() + 2, &tstart));
+  GRE_CHECK(ws_array(s, WS_COUNTERS, 3, &c));
+  GRE_CHECK(ws_array(s, WS_OUTBUF2, P, &call));
+  bc = (BfsCounters*)(c + 1);
+  err = (uint32_t*)(c + 2);
+  bcall = (BfsCounters*)call;
+  GRE_CHECK(prepare_output(s, dist, n, WS_OUTBUF, &dout));
+  void* cubtmp = nullptr;
+  size_t cubbytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, cubbytes, deg, prefix, L + 1, s->stream);
+  GRE_CHECK(s->ws.get(WS_CUB, cubbytes, &cubtmp));
+
+  RunTimer timer(s);
+  uint32_t xr = 0;
+  GRE_CUDA(cudaMemcpyAsync(&xr, p->xof + src, sizeof xr, cudaMemcpyDeviceToHost, s->stream));
+  GRE_CUDA(cudaMemsetAsync(dl, 0xff, sizeof(uint32_t) * L, s->stream));
+  GRE_CUDA(cudaMemsetAsync(pend, 0, sizeof(uint32_t) * W, s->stream));
+  GRE_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), s->stream));
+  GRE_CUDA(cudaStreamSynchronize(s->stream));
+  if (xr / L == me) {
+    const uint32_t slot = xr - (uint32_t)(me * L), zero = 0, bit = 1u << (slot & 31u);
+    GRE_CUDA(cudaMemcpyAsync(dl + slot, &zero, sizeof zero, cudaMemcpyHostToDevice, s->stream));
+    GRE_CUDA(cudaMemcpyAsync(pend + (slot >> 5), &bit, sizeof bit, cudaMemcpyHostToDevice, s->stream));
+  }
+  // Supersteps of the reference's SSSP (every improved vertex scatters dist + w, combine = min),
+  // ordered near-far: only pending slots below a global limit scatter; when none is left
+  // anywhere, the limit moves to the smallest pending distance + delta (half the mean weight).
+  const uint32_t delta = p->delta ? p->delta : 0xffffffffu;
+  uint32_t limit = delta;
+  uint64_t relaxed = 0, bytes = 0;
+  uint32_t steps = 0;
+  std::vector<SsspCounters> h(P);
+  for (;;) {
+    const SsspCounters zero{0, 0, 0xffffffffffffffffull, 0};
+    GRE_CUDA(cudaMemcpyAsync(c, &zero, sizeof zero, cudaMemcpyHostToDevice, s->stream));
+    k_part_sssp_select<<<grid_for(W, 256), 256, 0, s->stream>>>(W, pend, dl, limit, s->outdeg, queue, c);
+    GRE_LAUNCH_CHECK();
+    GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLGATHER, c, call, sizeof(SsspCounters)));
+    GRE_CUDA(cudaMemcpyAsync(h.data(), call, sizeof(SsspCounters) * P, cudaMemcpyDeviceToHost, s->stream));
+    GRE_CUDA(cudaStreamSynchronize(s->stream));
+    uint64_t near = 0, pending = 0, min_far = ~0ull;
+    for (const SsspCounters& x : h) {
+      near += x.near;
+      pending += x.pending;
+      min_far = std::min<uint64_t>(min_far, x.min_far);
+    }
+    bytes += 4 * W + 8 * (h[me].near + h[me].pending);
+    if (near == 0) {
+      if (pending == 0) break;
+      // every rank sees the same sums: the same new limit
+      limit = min_far > 0xffffffffull - delta ? 0xffffffffu : (uint32_t)(min_far + delta);
+      continue;
+    }
+    const uint64_t nq = h[me].near;
+    GRE_CUDA(cudaMemsetAsync(cand, 0xff, sizeof(uint32_t) * P * L, s->stream));
+    unsigned long long total = h[me].arcs;
+    if (nq && total) {  // the one-GPU path's tile relaxation: offers go to cand, owners' distances from dl
+      k_frontier_degrees<<<grid_for(nq, 256), 256, 0, s->stream>>>(queue, nq, s->off, deg);
+      GRE_CUDA(cub::DeviceScan::ExclusiveSum(cubtmp, cubbytes, deg, prefix, nq + 1, s->stream));
+      GRE_CHECK(sssp_relax_tiles(s->stream, queue, nq, prefix, total, tstart, s->off, s->col, p->w32, dl, cand, nullptr, err));
+    }
+    GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLTOALL, cand, recv, 4 * L));
+    k_part_sssp_claim<<<grid_for(L, 256), 256, 0, s->stream>>>(L, P, recv, dl, s->outdeg, pend);
+    GRE_LAUNCH_CHECK();
+    relaxed += total;
+    bytes += 16 * nq + 12 * total + 4 * P * L * 3 + 4 * L;
+    ++steps;
+    stats_record(st, near);
+  }
+  GRE_CUDA(cudaMemsetAsync(bc, 0, sizeof(BfsCounters), s->stream));
+  k_part_reached_dist<<<grid_for(L, 256), 256, 0, s->stream>>>(L, dl, s->outdeg, &bc->next_arcs);
+  GRE_LAUNCH_CHECK();
+  BfsCounters sum;
+  GRE_CHECK(exchange_counters(p, xchg, ctx, bc, bcall, &sum, nullptr));
+  GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLGATHER, dl, dist_all, 4 * L));
+  k_part_out<uint32_t><<<grid_for(P * L, 256), 256, 0, s->stream>>>(P * L, p->xmap, dist_all, dout);
+  GRE_LAUNCH_CHECK();
+  // checked after the last collective, so that every rank takes the same ones
+  uint32_t herr = 0;
+  GRE_CUDA(cudaMemcpyAsync(&herr, err, sizeof herr, cudaMemcpyDeviceToHost, s->stream));
+  GRE_CUDA(cudaStreamSynchronize(s->stream));
+  if (herr) {
+    set_error("gre_part_sssp: frontier tile overflow");
+    return GRE_FAILURE;
+  }
+  GRE_CHECK(finish_output(s, dist, dout, n));
+  GRE_CHECK(timer.stop(st));
+  if (st) {
+    st->supersteps = steps;
+    st->arcs_traversed = relaxed;  // this rank's
+    st->traversed_edges = s->symmetric() ? sum.next_arcs / 2 : sum.next_arcs;
+    st->algo_bytes = bytes;
+  }
+  return GRE_SUCCESS;
+}
+
+int gre_part_cc(gre_part p, uint32_t* label, gre_exchange_fn xchg, void* ctx, gre_stats* st) {
+  if (!p || !label || !xchg) return GRE_NULL;
+  gre_graph s = p->sub;
+  GRE_CHECK(use_graph(s));
+  stats_reset(st);
+  const uint64_t n = p->n, P = p->nparts, L = p->L, me = p->rank;
+  uint32_t *lab, *lab_all, *dout;
+  BfsCounters *c, *call;
+  GRE_CHECK(ws_array(s, WS_A, L, &lab));
+  GRE_CHECK(ws_array(s, WS_B, P * L, &lab_all));
+  GRE_CHECK(ws_array(s, WS_COUNTERS, 1, &c));
+  GRE_CHECK(ws_array(s, WS_OUTBUF2, P, &call));
+  GRE_CHECK(prepare_output(s, label, n, WS_OUTBUF, &dout));
+  RunTimer timer(s);
+  k_part_cc_init<<<grid_for(L, 256), 256, 0, s->stream>>>(L, p->xmap + me * L, lab);
+  GRE_LAUNCH_CHECK();
+  // label propagation to the smallest caller id with shortcuts (min over in-arcs, and over
+  // out-arcs too on a directed graph: weak components, as gre_cc); rows split by the degree bins
+  // (bins 0-5 one to 32 lanes per row, 6-7 CTA per row)
+  auto sweep = [&](const DegreeBins& B, const uint64_t* off, const uint32_t* col) {
+    const uint64_t nbig = B.count[6] + B.count[7];
+    auto lanes = [&](auto kernel, int b, int G) {
+      if (B.count[b])
+        kernel<<<grid_for(B.count[b] * G, 256, 8), 256, 0, s->stream>>>(B.rows + B.start[b], B.count[b], off, col, lab_all, p->xof,
+                                                                          lab, c);
+    };
+    lanes(k_part_cc_lanes<1>, 0, 1);
+    lanes(k_part_cc_lanes<2>, 1, 2);
+    lanes(k_part_cc_lanes<4>, 2, 4);
+    lanes(k_part_cc_lanes<8>, 3, 8);
+    lanes(k_part_cc_lanes<16>, 4, 16);
+    lanes(k_part_cc_lanes<32>, 5, 32);
+    if (nbig)
+      k_part_cc_rows<<<grid_for(nbig * 256, 256, 8), 256, 0, s->stream>>>(B.rows + B.start[6], nbig, off, col, lab_all, p->xof,
+                                                                            lab, c);
+  };
+  uint32_t steps = 0;
+  uint64_t bytes = 0;
+  BfsCounters sum;
+  for (;;) {
+    GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLGATHER, lab, lab_all, 4 * L));
+    GRE_CUDA(cudaMemsetAsync(c, 0, sizeof(BfsCounters), s->stream));
+    sweep(s->bins_in, s->roff, s->rcol);
+    if (s->roff != s->off) sweep(s->bins_out, s->off, s->col);
+    GRE_LAUNCH_CHECK();
+    GRE_CHECK(exchange_counters(p, xchg, ctx, c, call, &sum, nullptr));
+    ++steps;
+    bytes += 8 * (L + 1) + 8 * (p->arcs_in + (s->roff != s->off ? p->arcs_out : 0)) + 4 * P * L + 8 * L;
+    stats_record(st, sum.next_count);
+    if (sum.next_count == 0) break;
+  }
+  GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLGATHER, lab, lab_all, 4 * L));
+  k_part_out<uint32_t><<<grid_for(P * L, 256), 256, 0, s->stream>>>(P * L, p->xmap, lab_all, dout);
+  GRE_LAUNCH_CHECK();
+  GRE_CHECK(finish_output(s, label, dout, n));
+  GRE_CHECK(timer.stop(st));
+  if (st) {
+    st->supersteps = steps;
+    st->arcs_traversed = (p->arcs_in + (s->roff != s->off ? p->arcs_out : 0)) * (uint64_t)steps;
+    st->traversed_edges = s->symmetric() ? p->m / 2 : p->m;
+    st->algo_bytes = bytes;
   }
   return GRE_SUCCESS;
 }

@@ -110,11 +110,16 @@ __global__ void k_tile_starts(const uint64_t* __restrict__ prefix, uint64_t nq, 
   }
 }
 
+// OFFER: the owners' distances come from srcdist and the improved heads are not recorded (the
+// partitioned path offers to a separate candidate array); otherwise from dist itself, with a
+// changed bit per improved head.
+template <bool OFFER>
 __global__ void __launch_bounds__(kTileThreads) k_sssp_relax(const uint32_t* __restrict__ queue, uint64_t nq,
                                                              const uint64_t* __restrict__ prefix, uint64_t total, const uint32_t* __restrict__ start,
                                                              const uint64_t* __restrict__ base, const uint32_t* __restrict__ col,
-                                                             const uint32_t* __restrict__ w, uint32_t* __restrict__ dist,
-                                                             uint32_t* __restrict__ changed, uint32_t* __restrict__ error) {
+                                                             const uint32_t* __restrict__ w, const uint32_t* __restrict__ srcdist,
+                                                             uint32_t* __restrict__ dist, uint32_t* __restrict__ changed,
+                                                             uint32_t* __restrict__ error) {
   using OwnerScan = cub::BlockScan<uint32_t, kTileThreads>;
   __shared__ uint64_t s_arc[kTile + 1];                // arc index at tile position s_rel[j]
   __shared__ uint32_t s_du[kTile + 1];                 // distance of owner j
@@ -139,7 +144,7 @@ __global__ void __launch_bounds__(kTileThreads) k_sssp_relax(const uint32_t* __r
       const uint64_t r = p > t0 ? p - t0 : 0;
       s_rel[j] = (uint16_t)r;
       s_arc[j] = base[u] + (t0 + r - p);
-      s_du[j] = __ldcg(dist + u);
+      s_du[j] = __ldcg((OFFER ? srcdist : dist) + u);
     }
     __syncthreads();
     // owner of every tile position: mark where each owner's arcs begin, then a running maximum
@@ -186,7 +191,7 @@ __global__ void __launch_bounds__(kTileThreads) k_sssp_relax(const uint32_t* __r
       const uint32_t nd = du[k] + wt[k];
       if (ok && nd < dv[k]) {
         atomicMin(dist + v[k], nd);
-        atomicOr(changed + (v[k] >> 5), 1u << (v[k] & 31u));
+        if (!OFFER) atomicOr(changed + (v[k] >> 5), 1u << (v[k] & 31u));
       }
     }
     __syncthreads();
@@ -317,7 +322,7 @@ struct AddU64 {
 // Bucket width of the near-far split.  Default: half the mean arc weight (unit weights give
 // one bucket per BFS level); 0 relaxes every improved vertex at once (Bellman-Ford frontier).
 // The GRE_SSSP_DELTA environment variable overrides it.
-static int sssp_delta(gre_graph g, uint32_t* delta) {
+int sssp_delta(gre_graph g, uint32_t* delta) {
   if (const char* e = getenv("GRE_SSSP_DELTA")) {
     *delta = (uint32_t)strtoul(e, nullptr, 10);
     return GRE_SUCCESS;
@@ -350,14 +355,38 @@ static int init_counters(gre_graph g, uint32_t* cnt, uint32_t near, uint32_t nfa
 
 // Resident CTAs of the relaxation kernel per SM: the grid is exactly one wave, so that no
 // CTA starts its tiles late.
+template <bool OFFER>
 static int relax_blocks_per_sm() {
   static int per_sm = 0;
   if (!per_sm) {
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sssp_relax, kTileThreads, 0) != cudaSuccess || b < 1) b = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_sssp_relax<OFFER>, kTileThreads, 0) != cudaSuccess || b < 1) b = 1;
     per_sm = b;
   }
   return per_sm;
+}
+
+uint64_t sssp_tile_arcs() { return kTile; }
+
+// The relaxation of one frontier pass: tile starts, then k_sssp_relax over one wave of CTAs.
+int sssp_relax_tiles(cudaStream_t stream, const uint32_t* queue, uint64_t nq, const uint64_t* prefix, uint64_t total,
+                     uint32_t* tstart, const uint64_t* base, const uint32_t* col, const uint32_t* w, const uint32_t* srcdist,
+                     uint32_t* dist, uint32_t* changed, uint32_t* error) {
+  if (!total) return GRE_SUCCESS;
+  const uint64_t ntiles = (total + kTile - 1) / kTile;
+  k_tile_starts<<<grid_for(nq, 256), 256, 0, stream>>>(prefix, nq, tstart);
+  // the arc count is a launch argument: read inside the kernel instead, the relaxation
+  // measured 1.7x slower on RMAT-26
+  const bool offer = srcdist != dist;
+  const int grid = (int)std::min<uint64_t>(ntiles, (uint64_t)num_sms() * (offer ? relax_blocks_per_sm<true>() : relax_blocks_per_sm<false>()));
+  if (!offer)
+    k_sssp_relax<false><<<grid, kTileThreads, 0, stream>>>(queue, nq, prefix, total, tstart, base, col, w, nullptr, dist, changed,
+                                                           error);
+  else
+    k_sssp_relax<true><<<grid, kTileThreads, 0, stream>>>(queue, nq, prefix, total, tstart, base, col, w, srcdist, dist, nullptr,
+                                                          error);
+  GRE_LAUNCH_CHECK();
+  return GRE_SUCCESS;
 }
 
 // Light/heavy split of the arcs for bucket width delta (built once per graph, weights and delta).
@@ -421,7 +450,6 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
   uint32_t* far = fa;
   uint32_t* far2 = fb;
   uint32_t steps = 0;
-  const int sms = num_sms();
   uint32_t h[8];
   auto read_counters = [&]() -> int {
     GRE_CUDA(cudaMemcpyAsync(h, cnt, sizeof h, cudaMemcpyDeviceToHost, g->stream));
@@ -449,13 +477,8 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
     GRE_CUDA(cudaStreamSynchronize(g->stream));
     GRE_CHECK(init_counters(g, cnt, 0, (uint32_t)nfar, (uint32_t)nb));
     if (total) {
-      const uint64_t ntiles = (total + kTile - 1) / kTile;
-      k_tile_starts<<<grid_for(nlist, 256), 256, 0, g->stream>>>(prefix, nlist, tstart);
-      // the arc count is a launch argument: read inside the kernel instead, the relaxation
-      // measured 1.7x slower on RMAT-26
-      const int grid = (int)std::min<uint64_t>(ntiles, (uint64_t)sms * relax_blocks_per_sm());
-      k_sssp_relax<<<grid, kTileThreads, 0, g->stream>>>(list, nlist, prefix, total, tstart, heavy ? lend : off, col, w, dist,
-                                                          changed, cnt + 1);
+      GRE_CHECK(sssp_relax_tiles(g->stream, list, nlist, prefix, total, tstart, heavy ? lend : off, col, w, dist, dist, changed,
+                                 cnt + 1));
       k_sssp_classify<<<grid_for(nwords, 256, 8), 256, 0, g->stream>>>(nwords, changed, dist, off, lend, limit, out_near, infar,
                                                                         far, inbucket, blist, cnt);
     }

@@ -11,7 +11,7 @@
 // weight function (environment GRE_WSEED, default 1) instead of unseeded rand(); BC runs all
 // roots of the file and accumulates them.  Exit status 0 on success, the gre status otherwise.
 //
-//   gre_run <part_bfs|part_pagerank|part_pagerank_iter> <prefix> --ranks P --rank r --id-file F [--device d]
+//   gre_run <part_bfs|part_sssp|part_cc|part_pagerank|part_pagerank_iter> <prefix> --ranks P --rank r --id-file F [--device d]
 //
 // One rank of an np = P job over P GPUs (the reference's mpirun -np P): every rank loads the
 // graph, keeps its part (gre/gre.hpp PartitionedGraph) and runs over the library's NCCL
@@ -57,6 +57,11 @@ static std::vector<uint8_t> shared_id(const std::string& path, int rank) {
 }
 
 static int run_partitioned(const std::string& algo, const std::string& prefix, int argc, char** argv) {
+  if (algo != "part_bfs" && algo != "part_sssp" && algo != "part_cc" && algo != "part_pagerank" &&
+      algo != "part_pagerank_iter") {
+    fprintf(stderr, "unknown algorithm %s\n", algo.c_str());
+    return 2;
+  }
   int ranks = 1, rank = 0, device = 0;
   std::string id_file;
   for (int i = 3; i + 1 < argc; i += 2) {
@@ -78,10 +83,15 @@ static int run_partitioned(const std::string& algo, const std::string& prefix, i
   gre_stats st{};
   {
     gre::DistributedGraph g;
-    if (algo == "part_bfs") g.ingress<gre::InOut>(prefix, "ascii", "edgelists", false, true, device);
+    if (algo == "part_bfs" || algo == "part_cc") g.ingress<gre::InOut>(prefix, "ascii", "edgelists", false, true, device);
     else g.ingress<gre::Out>(prefix, "ascii", "edgelists", false, true, device);
+    if (algo == "part_sssp") {
+      const char* ws = getenv("GRE_WSEED");
+      g.loadEdgePropertyHash(ws ? strtoull(ws, nullptr, 10) : 1);
+    }
     gre::PartitionedGraph part(g, comm);
-    if (algo == "part_bfs") {
+    uint32_t root = 0;
+    if (algo == "part_bfs" || algo == "part_sssp") {
       std::vector<uint32_t> roots(1024);
       uint32_t nroots = 0;
       int s = gre_read_roots(prefix.c_str(), roots.data(), (uint32_t)roots.size(), &nroots);
@@ -89,11 +99,29 @@ static int run_partitioned(const std::string& algo, const std::string& prefix, i
         fprintf(stderr, "Err in reading src vertex from file.\n");
         return s ? s : GRE_IO_ERROR;
       }
-      std::vector<int32_t> level = part.bfs(roots[0], &st);
+      root = roots[0];
+    }
+    if (algo == "part_bfs") {
+      std::vector<int32_t> level = part.bfs(root, &st);
       print_supersteps(st);
       long reached = 0;
       for (int32_t l : level) reached += l >= 0;
       printf("Reached vertices: %ld\n", reached);
+    } else if (algo == "part_sssp") {
+      std::vector<uint32_t> dist = part.sssp(root, &st);
+      long reached = 0;
+      unsigned long long total = 0;
+      for (uint32_t d : dist)
+        if (d != 0xffffffffu) {
+          ++reached;
+          total += d;
+        }
+      printf("Reached vertices: %ld\nSum of distances: %llu\n", reached, total);
+    } else if (algo == "part_cc") {
+      std::vector<uint32_t> label = part.cc(&st);
+      long comps = 0;
+      for (size_t v = 0; v < label.size(); ++v) comps += label[v] == v;
+      printf("Number of components: %ld\n", comps);
     } else {
       std::vector<double> pr = part.pagerank(algo == "part_pagerank_iter", 0.85, algo == "part_pagerank" ? 10 : 20, &st);
       double sum = 0;
@@ -109,7 +137,7 @@ static int run_partitioned(const std::string& algo, const std::string& prefix, i
 int main(int argc, char** argv) {
   if (argc < 3) {
     fprintf(stderr, "usage: %s pagerank|pagerank_iter|pagerank_delta|bfs|sssp|sssp1|cc|cin|bc prefix [ascii] [edgelists]\n"
-                    "       %s part_bfs|part_pagerank|part_pagerank_iter prefix --ranks P --rank r --id-file F [--device d]\n",
+                    "       %s part_bfs|part_sssp|part_cc|part_pagerank|part_pagerank_iter prefix --ranks P --rank r --id-file F [--device d]\n",
             argv[0], argv[0]);
     return 2;
   }

@@ -149,6 +149,8 @@ def lib() -> C.CDLL:
             "gre_part_layout": (I32, [U64, U32, C.POINTER(U64), P]),
             "gre_part_bfs": (I32, [P, U32, P, EXCHANGE_FN, P, S]),
             "gre_part_pagerank": (I32, [P, I32, D, U32, P, EXCHANGE_FN, P, S]),
+            "gre_part_sssp": (I32, [P, U32, P, EXCHANGE_FN, P, S]),
+            "gre_part_cc": (I32, [P, P, EXCHANGE_FN, P, S]),
             "gre_rmat_host": (I32, [U32, U32, U64, I32, C.POINTER(U64), C.POINTER(U64), C.POINTER(P), C.POINTER(P)]),
             "gre_host_free": (None, [P]),
             "gre_write_edgelists": (I32, [C.c_char_p, U64, U64, P, P, U32]),

@@ -1,4 +1,5 @@
-"""1D-partitioned single-source paths: one graph split by vertex over ranks, one GPU per rank.
+"""1D-partitioned single-source paths (BFS, PageRank, SSSP, CC): one graph split by vertex over
+ranks, one GPU per rank.
 
 The reference spreads one graph over MPI ranks (vertex placement, GraphIngress.hpp:1126-1450)
 and runs every superstep as sync scatters -> local compute -> sync combiners -> apply
@@ -9,6 +10,8 @@ in- and out-arcs of its own vertices, and the exchanges are
 * PageRank: an all-gather of the owners' contributions every superstep (8 bytes per vertex);
 * BFS bottom-up level: an all-gather of the owners' frontier bits (n/8 bytes);
 * BFS top-down level: an all-to-all of candidate bitmaps (each owner ORs the blocks it gets),
+* SSSP superstep: an all-to-all of candidate distances (each owner keeps the smallest offer),
+* CC superstep: an all-gather of the labels (4 bytes per vertex),
 
 plus a 32-byte all-gather of the level counters.  The library calls back into the host for each
 collective (``gre_exchange_fn``); this module supplies three implementations:
@@ -273,6 +276,25 @@ class Part:
         (cb.check if cb is not None else G._check)(status, "gre_part_bfs")
         return out, G.Stats._from(st)
 
+    def sssp(self, src: int, exchange, out=None):
+        """Distances of all n vertices (caller order) from caller vertex `src` (0xffffffff
+        unreached), with the uint32 weights the graph had when the part was made."""
+        out = G._out(out, self.n, np.uint32)
+        st = G._stats()
+        cfn, ctx, cb = self._exchange(exchange)
+        status = G.lib().gre_part_sssp(self._h, int(src), G._ptr(out), cfn, ctx, C.byref(st))
+        (cb.check if cb is not None else G._check)(status, "gre_part_sssp")
+        return out, G.Stats._from(st)
+
+    def cc(self, exchange, out=None):
+        """Component labels of all n vertices (smallest caller id of the weak component)."""
+        out = G._out(out, self.n, np.uint32)
+        st = G._stats()
+        cfn, ctx, cb = self._exchange(exchange)
+        status = G.lib().gre_part_cc(self._h, G._ptr(out), cfn, ctx, C.byref(st))
+        (cb.check if cb is not None else G._check)(status, "gre_part_cc")
+        return out, G.Stats._from(st)
+
     def pagerank(self, exchange, variant: int = G.PR_ITER, d: float = 0.85, iters: int = 20, out=None):
         """PageRank of all n vertices (caller order), as :func:`graphine_b200.gre.pagerank`."""
         out = G._out(out, self.n, np.float64)
@@ -331,6 +353,30 @@ def bfs(g: "G.Graph", src: int, group=None, exchange=None):
     p = Part(g, x.world, x.rank)
     try:
         return p.bfs(src, x)
+    finally:
+        p.free()
+        if exchange is None:
+            x.free()
+
+
+def sssp(g: "G.Graph", src: int, group=None, exchange=None):
+    """SSSP distances over the ranks of `group` (as :func:`bfs`)."""
+    x = exchange if exchange is not None else NcclExchange(group)
+    p = Part(g, x.world, x.rank)
+    try:
+        return p.sssp(src, x)
+    finally:
+        p.free()
+        if exchange is None:
+            x.free()
+
+
+def cc(g: "G.Graph", group=None, exchange=None):
+    """Component labels over the ranks of `group` (as :func:`bfs`)."""
+    x = exchange if exchange is not None else NcclExchange(group)
+    p = Part(g, x.world, x.rank)
+    try:
+        return p.cc(x)
     finally:
         p.free()
         if exchange is None:

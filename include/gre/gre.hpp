@@ -242,6 +242,16 @@ class PartitionedGraph {
     check(gre_part_bfs(p_, src, level.data(), gre_nccl_exchange, comm_.handle(), st), "gre_part_bfs");
     return level;
   }
+  std::vector<uint32_t> sssp(uint32_t src, gre_stats* st = nullptr) {
+    std::vector<uint32_t> dist(n_);
+    check(gre_part_sssp(p_, src, dist.data(), gre_nccl_exchange, comm_.handle(), st), "gre_part_sssp");
+    return dist;
+  }
+  std::vector<uint32_t> cc(gre_stats* st = nullptr) {
+    std::vector<uint32_t> label(n_);
+    check(gre_part_cc(p_, label.data(), gre_nccl_exchange, comm_.handle(), st), "gre_part_cc");
+    return label;
+  }
   std::vector<double> pagerank(bool iter, double d, uint32_t iters, gre_stats* st = nullptr) {
     std::vector<double> pr(n_);
     check(gre_part_pagerank(p_, iter ? GRE_PR_ITER : GRE_PR_REFERENCE, d, iters, pr.data(), gre_nccl_exchange,

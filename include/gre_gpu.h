@@ -243,7 +243,8 @@ int gre_pagerank_adjoint(gre_graph g, double d, const double* r, const double* c
                          gre_stats* st);
 
 /* ---------------------------------------------------------------------------------------
- * 1D-partitioned single-source paths: one graph split by vertex over P ranks, one GPU each.
+ * 1D-partitioned single-source paths (BFS, PageRank, SSSP, CC): one graph split by vertex over P
+ * ranks, one GPU each.
  * Replaces the np > 1 superstep of SynchronousEngine (sync scatters, Engine.hpp:273-315;
  * local compute; sync combiners, Engine.hpp:333-374; apply), with the vertex placement of
  * GraphIngress.hpp:1126-1450 replaced by a fixed one: internal ids dealt to ranks one by one in
@@ -277,6 +278,15 @@ int gre_part_bfs(gre_part p, uint32_t src, int32_t* level, gre_exchange_fn xchg,
 /* PageRank as gre_pagerank; every rank receives all n values. */
 int gre_part_pagerank(gre_part p, int variant, double d, uint32_t iters, double* pr,
                       gre_exchange_fn xchg, void* ctx, gre_stats* st);
+
+/* SSSP as gre_sssp (uint32 weights the graph had when the part was made); every rank receives
+ * all n distances.  Frontier Bellman-Ford supersteps: offers to remote heads go to their owners
+ * by one all-to-all per superstep, the owner keeps the smallest. */
+int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg, void* ctx,
+                  gre_stats* st);
+/* Connected components as gre_cc (label = smallest caller id of the weak component); every
+ * rank receives all n labels.  Label propagation with shortcuts, one all-gather per superstep. */
+int gre_part_cc(gre_part p, uint32_t* label, gre_exchange_fn xchg, void* ctx, gre_stats* st);
 
 /* The library's own exchange: NCCL on the part's stream (NCCL is loaded at the first
  * gre_nccl_unique_id / gre_nccl_create: libnccl.so.2 already in the process, else the

@@ -77,3 +77,16 @@ def test_partitioned_driver_one_rank(golden):
         for x in pr:  # the driver's order of summation
             s += float(x)
         assert f"Sum of pr: {s:.15g}" in p.stdout
+        wseed = int(case["wseed"])
+        p = subprocess.run([DRIVER, "part_sssp", prefix] + args, capture_output=True, text=True, timeout=300,
+                           env={**os.environ, "GRE_WSEED": str(wseed)})
+        assert p.returncode == 0, p.stderr
+        gs = G.Graph.ingress(prefix, dir=G.Out)
+        gs.set_weights_hash(wseed)
+        d, _ = G.sssp(gs, [int(case["roots"][0])])
+        fin = d[d != 0xFFFFFFFF].astype(np.int64)
+        assert f"Reached vertices: {len(fin)}" in p.stdout and f"Sum of distances: {int(fin.sum())}" in p.stdout
+        p = subprocess.run([DRIVER, "part_cc", prefix] + args, capture_output=True, text=True, timeout=300)
+        assert p.returncode == 0, p.stderr
+        lab, _ = G.cc(g)
+        assert f"Number of components: {int((lab == np.arange(n)).sum())}" in p.stdout

@@ -74,6 +74,68 @@ def test_partitioned_directed_graph(P):
         np.testing.assert_array_equal(pr, one)
 
 
+WSEED = 11
+
+
+@pytest.mark.parametrize("P", [1, 2, 3, 4])
+@pytest.mark.parametrize("reorder", [False, True], ids=["plain", "relabelled"])
+def test_partitioned_sssp_equals_oracle_and_one_gpu(P, reorder):
+    n, off, col, g = _graph(11, True, reorder)
+    g.set_weights_hash(WSEED)
+    R = O.Restatement.from_csr(n, off, col)
+    roots = G.sample_sources(off, 2, 5)
+    ref = R.sssp_many(roots, WSEED)
+    for i, s in enumerate(roots):
+        one, st1 = G.sssp(g, [s])
+        np.testing.assert_array_equal(one, ref[i])
+        for dist, st in PT.run_local(g, P, lambda part, x: part.sssp(int(s), x)):
+            np.testing.assert_array_equal(dist, ref[i])
+            assert st.traversed_edges == st1.traversed_edges
+
+
+@pytest.mark.parametrize("P", [1, 2, 3, 4])
+@pytest.mark.parametrize("reorder", [False, True], ids=["plain", "relabelled"])
+def test_partitioned_cc_equals_oracle_and_one_gpu(P, reorder):
+    n, off, col, g = _graph(11, True, reorder)
+    R = O.Restatement.from_csr(n, off, col)
+    ref, _ = R.cc()
+    one, _ = G.cc(g)
+    np.testing.assert_array_equal(one, ref)
+    assert len(np.unique(ref)) > 1  # several components (isolated vertices among them)
+    for lab, st in PT.run_local(g, P, lambda part, x: part.cc(x)):
+        np.testing.assert_array_equal(lab, ref)
+        assert st.active[-1] == 0
+
+
+@pytest.mark.parametrize("P", [2, 3])
+def test_partitioned_sssp_and_cc_directed(P):
+    n, off, col, g = _graph(10, False, True, seed=3)
+    g.set_weights_hash(WSEED)
+    R = O.Restatement.from_csr(n, off, col)
+    roots = G.sample_sources(off, 2, 9)
+    ref = R.sssp_many(roots, WSEED)
+    for i, s in enumerate(roots):
+        for dist, _ in PT.run_local(g, P, lambda part, x: part.sssp(int(s), x)):
+            np.testing.assert_array_equal(dist, ref[i])
+    one, _ = G.cc(g)  # weak components
+    for lab, _ in PT.run_local(g, P, lambda part, x: part.cc(x)):
+        np.testing.assert_array_equal(lab, one)
+
+
+def test_partitioned_sssp_needs_weights_at_creation():
+    n, off, col, g = _graph(9, True, False)
+    p = PT.Part(g, 1, 0)
+    g.set_weights_hash(WSEED)  # too late for this part
+    with pytest.raises(G.GreError) as e:
+        p.sssp(0, PT.LocalExchange(1).for_rank(0))
+    assert e.value.status == G.GRE_INVALID_ARG
+    p.free()
+    p = PT.Part(g, 1, 0)
+    dist, _ = p.sssp(0, PT.LocalExchange(1).for_rank(0))
+    np.testing.assert_array_equal(dist, G.sssp(g, [0])[0])
+    p.free()
+
+
 def test_parts_with_only_padding_and_isolated_source():
     # 5 vertices over 4 ranks: rank slots of 64, most of them padding
     n = 5
@@ -182,6 +244,7 @@ def test_library_nccl_exchange_one_rank():
     import torch
 
     n, off, col, g = _graph(12, True, True)
+    g.set_weights_hash(WSEED)
     x = PT.NcclExchange()
     p = PT.Part(g, 1, 0)
     try:
@@ -194,6 +257,8 @@ def test_library_nccl_exchange_one_rank():
             out = torch.empty(n, dtype=torch.float64, device="cuda")
             p.pagerank(x, variant, 0.85, 20, out=out)
             np.testing.assert_array_equal(out.cpu().numpy(), G.pagerank(g, variant, 0.85, 20)[0])
+        np.testing.assert_array_equal(p.cc(x)[0], G.cc(g)[0])
+        np.testing.assert_array_equal(p.sssp(17, x)[0], G.sssp(g, [17])[0])
     finally:
         p.free()
         x.free()
