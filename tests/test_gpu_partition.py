@@ -262,3 +262,20 @@ def test_library_nccl_exchange_one_rank():
     finally:
         p.free()
         x.free()
+
+
+def test_torch_exchange_stages_device_buffers_through_gloo():
+    import torch.distributed as dist
+
+    n, off, col, g = _graph(11, True, True)
+    g.set_weights_hash(WSEED)
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{_free_port()}", rank=0, world_size=1)
+    try:
+        x = PT.TorchExchange()  # device buffers, host staging (gloo has no device collectives here)
+        p = PT.Part(g, 1, 0)
+        np.testing.assert_array_equal(p.bfs(3, x)[0], G.bfs(g, [3])[0])
+        np.testing.assert_array_equal(p.sssp(3, x)[0], G.sssp(g, [3])[0])
+        np.testing.assert_array_equal(p.pagerank(x, G.PR_ITER, 0.85, 10)[0], G.pagerank(g, G.PR_ITER, 0.85, 10)[0])
+        p.free()
+    finally:
+        dist.destroy_process_group()
