@@ -38,6 +38,11 @@ REORDER = 0x20
 PR_REFERENCE, PR_ITER = 0, 1
 MAX_RECORDED = 1024
 XCHG_ALLGATHER, XCHG_ALLTOALL = 0, 1  # enum gre_exchange_kind
+BATCH_BFS, BATCH_CC, BATCH_PAGERANK = 0, 2, 3  # enum gre_batch_algo
+
+
+class BatchPageRankParams(C.Structure):
+    _fields_ = [("variant", C.c_int), ("d", C.c_double), ("iters", C.c_uint32)]
 # int (*gre_exchange_fn)(void* ctx, int kind, const void* send, void* recv, uint64_t bytes, void* stream)
 EXCHANGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p)
 
@@ -139,6 +144,7 @@ def lib() -> C.CDLL:
             "gre_ppr": (I32, [P, P, U32, D, U32, I32, P, S]),
             "gre_pagerank_weighted": (I32, [P, D, P, D, U32, P, S]),
             "gre_pagerank_adjoint": (I32, [P, D, P, P, D, U32, P, P, P, S]),
+            "gre_graph_batch_run": (I32, [P, U32, I32, P, P, S]),
             "gre_part_create": (I32, [P, U32, U32, C.POINTER(P)]),
             "gre_part_free": (I32, [P]),
             "gre_part_info": (I32, [P, C.POINTER(U64), C.POINTER(U64), C.POINTER(U64)]),
@@ -515,6 +521,29 @@ def pagerank_adjoint(g: Graph, r, c, d: float = 0.85, tol: float = 1e-14, max_it
 # ----------------------------------------------------------------------------------------------
 # host utilities (no GPU)
 # ----------------------------------------------------------------------------------------------
+def graph_batch_run(graphs: Sequence[Graph], algo: int, roots=None, variant: int = PR_ITER, d: float = 0.85,
+                    iters: int = 20, outs=None):
+    """gre_graph_batch_run: one algorithm over k graphs in one launch sequence; returns the
+    per-graph result arrays (member ids) and the stats of the run over their union."""
+    k = len(graphs)
+    dt = np.float64 if algo == BATCH_PAGERANK else (np.int32 if algo == BATCH_BFS else np.uint32)
+    outs = [np.empty(g.n, dtype=dt) for g in graphs] if outs is None else list(outs)
+    arr = (C.c_void_p * k)(*[g._h.value for g in graphs])
+    optr = (C.c_void_p * k)(*[_ptr(o) for o in outs])
+    keep = None
+    if algo == BATCH_BFS:
+        keep = _as(roots, np.uint32)
+        par = _ptr(keep)
+    elif algo == BATCH_PAGERANK:
+        keep = BatchPageRankParams(variant, d, iters)
+        par = C.addressof(keep)
+    else:
+        par = None
+    st = _stats()
+    _check(lib().gre_graph_batch_run(arr, k, algo, par, optr, C.byref(st)), "gre_graph_batch_run")
+    return outs, Stats._from(st)
+
+
 def rmat_host(scale: int, edgefactor: int = 16, seed: int = 1, symmetric: bool = True):
     """Seeded RMAT CSR on the host: (n, row_off uint64[n+1], col uint32[m])."""
     n, m = C.c_uint64(), C.c_uint64()

@@ -242,6 +242,23 @@ int gre_pagerank_adjoint(gre_graph g, double d, const double* r, const double* c
                          uint32_t max_iters, double* lambda, double* grad_pers, double* grad_w,
                          gre_stats* st);
 
+/* Batches of k graphs of uneven size as one launch sequence: the members' block-diagonal union
+ * (gre_graph_union: unrelabelled members, same device) runs the algorithm once, every superstep
+ * covering all members; outs[i] receives member i's results (n_i entries, member ids, host or
+ * device memory).  Replaces the reference's per-graph driver loop.
+ *   GRE_BATCH_BFS       params: uint32_t roots[k] (member ids); outs: int32 levels
+ *   GRE_BATCH_CC        params: unused;                        outs: uint32 labels (member ids)
+ *   GRE_BATCH_PAGERANK  params: gre_batch_pagerank_params;     outs: double ranks
+ * st: the run over the union (its construction is not timed). */
+enum gre_batch_algo { GRE_BATCH_BFS = 0, GRE_BATCH_CC = 2, GRE_BATCH_PAGERANK = 3 };
+typedef struct {
+  int variant; /* gre_pr_variant */
+  double d;
+  uint32_t iters;
+} gre_batch_pagerank_params;
+int gre_graph_batch_run(const gre_graph* graphs, uint32_t k, int algo, const void* params,
+                        void** outs, gre_stats* st);
+
 /* ---------------------------------------------------------------------------------------
  * 1D-partitioned single-source paths (BFS, PageRank, SSSP, CC): one graph split by vertex over P
  * ranks, one GPU each.

@@ -96,3 +96,34 @@ def test_zero_sources_and_zero_seeds():
     assert not b.any()
     out, _ = G.ppr(g, np.zeros(0, np.uint32))
     assert out.size == 0
+
+
+def test_graph_batch_run_equals_per_graph_calls():
+    import torch
+
+    scales = [9, 12, 7, 11, 10]
+    gs, roots = [], []
+    for i, s in enumerate(scales):
+        n, off, col = G.rmat_host(s, 8, 40 + i, True)
+        gs.append(G.Graph.from_csr(n, off, col, dir=G.InOut, symmetric=True))
+        roots.append(int(G.sample_sources(off, 1, i)[0]))
+    dev_out = torch.empty(gs[1].n, dtype=torch.int32, device="cuda")
+    outs = [np.empty(g.n, np.int32) for g in gs]
+    outs[1] = dev_out
+    lv, st = G.graph_batch_run(gs, G.BATCH_BFS, roots=roots, outs=outs)
+    for g, r, x in zip(gs, roots, lv):
+        got = x.cpu().numpy() if hasattr(x, "cpu") else x
+        np.testing.assert_array_equal(got, G.bfs(g, [r])[0])
+    assert st.supersteps > 0
+    lab, _ = G.graph_batch_run(gs, G.BATCH_CC)
+    for g, x in zip(gs, lab):
+        np.testing.assert_array_equal(x, G.cc(g)[0])
+    pr, _ = G.graph_batch_run(gs, G.BATCH_PAGERANK, variant=G.PR_ITER, d=0.85, iters=20)
+    for g, x in zip(gs, pr):
+        assert rel_l1(x, G.pagerank(g, G.PR_ITER, 0.85, 20)[0]) <= 1e-12
+    with pytest.raises(G.GreError) as e:
+        G.graph_batch_run(gs, G.BATCH_BFS, roots=[r + 10**6 for r in roots])
+    assert e.value.status == G.GRE_INVALID_ARG
+    with pytest.raises(G.GreError) as e:
+        G.graph_batch_run(gs, 7)
+    assert e.value.status == G.GRE_INVALID_ARG
