@@ -2,7 +2,9 @@
 
 Checked against: the FP64 restatement (oracle), a dense FP64 solve of (I - d P^T) r = (1-d) w
 and (I - d P) lambda = c at small scale, and FP64 central finite differences of the GPU
-forward on random edges.  Tolerance 1e-6 relative for gradients.
+forward on random edges.  Tolerance 1e-6 relative for gradients.  The forward/adjoint pair is
+also wrapped in a torch.autograd.Function here (and only here) for torch.autograd.gradcheck and
+autograd gradients against the dense solve.
 """
 import numpy as np
 import pytest
@@ -102,3 +104,64 @@ def test_adjoint_vs_central_differences():
     p1[e] += 1.0
     r1, _, _ = G.pagerank_weighted(g, D, p1, tol=1e-16, max_iters=3000)
     assert abs(float(c @ r1) - float(c @ r) - gp[e]) <= 1e-9 * max(1.0, abs(gp[e]))
+
+
+def _pagerank_function():
+    """The adjoint behind a torch.autograd.Function (gradient-check harness only): forward sets
+    the arc weights and solves the weighted PageRank on the GPU, backward solves the transposed
+    fixed point with the incoming gradient as c (gre_pagerank_adjoint)."""
+    import torch
+
+    class WeightedPageRank(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, w, pers, g):
+            wd = w.detach().cpu().contiguous()
+            g.set_weights_f64(wd.numpy())
+            r, _, _ = G.pagerank_weighted(g, D, pers.detach().cpu().numpy(), tol=1e-16, max_iters=5000)
+            ctx.g = g
+            ctx.save_for_backward(wd.clone(), torch.from_numpy(r.copy()))
+            return torch.from_numpy(r.copy())
+
+        @staticmethod
+        def backward(ctx, grad_r):
+            wd, r = ctx.saved_tensors
+            ctx.g.set_weights_f64(wd.numpy())  # other forward calls may have changed the graph's weights
+            _, gp, gw, _, _ = G.pagerank_adjoint(ctx.g, r.numpy(), grad_r.contiguous().numpy(), D, tol=1e-16,
+                                                 max_iters=5000)
+            return torch.from_numpy(gw.copy()), torch.from_numpy(gp.copy()), None
+
+    return WeightedPageRank
+
+
+def test_autograd_function_gradcheck():
+    """torch.autograd.gradcheck of the wrapped forward/adjoint pair (FP64 central differences on
+    every arc weight and personalisation entry of a small weighted graph)."""
+    import torch
+
+    n, off, col, w, g = weighted_graph(5, 13, directed=True)
+    fn = _pagerank_function()
+    wt = torch.tensor(w, dtype=torch.float64, requires_grad=True)
+    pers = torch.tensor(np.random.default_rng(3).random(n) + 0.5, dtype=torch.float64, requires_grad=True)
+    assert torch.autograd.gradcheck(lambda a, b: fn.apply(a, b, g), (wt, pers), eps=1e-6, atol=1e-7, rtol=1e-5)
+
+
+def test_autograd_function_matches_dense_gradient():
+    import torch
+
+    n, off, col, w, g = weighted_graph(9, 21)
+    fn = _pagerank_function()
+    rng = np.random.default_rng(8)
+    c = torch.tensor(rng.standard_normal(n))
+    wt = torch.tensor(w, dtype=torch.float64, requires_grad=True)
+    pers = torch.ones(n, dtype=torch.float64, requires_grad=True)
+    loss = (c * fn.apply(wt, pers, g)).sum()
+    gw, gp = torch.autograd.grad(loss, (wt, pers))
+    P = dense_P(n, off, col, w)
+    I = np.eye(n)
+    r_ref = np.linalg.solve(I - D * P.T, (1 - D) * np.ones(n))
+    lam = np.linalg.solve(I - D * P, c.numpy())
+    src = np.repeat(np.arange(n), np.diff(off.astype(np.int64)))
+    s = np.bincount(src, weights=w, minlength=n)
+    gw_ref = D * r_ref[src] / s[src] * (lam[col] - (P @ lam)[src])
+    assert rel_l1(gw.numpy(), gw_ref) <= 1e-6
+    assert rel_l1(gp.numpy(), (1 - D) * lam) <= 1e-6
