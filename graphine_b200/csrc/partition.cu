@@ -1,4 +1,5 @@
-// 1D-partitioned single-source paths: one graph split by vertex over P ranks, one GPU each.
+// 1D-partitioned single-source paths (BFS, PageRank, SSSP, CC): one graph split by vertex over P
+// ranks, one GPU each.
 //
 // The reference at np > 1 gives every vertex one master rank (GraphIngress.hpp:1126-1450) and
 // runs a superstep as: sync scatters (masters send their scatter values to the ranks that read
@@ -15,9 +16,15 @@
 //   * BFS, top-down level: each rank expands its own frontier along out-arcs into a candidate
 //     bitmap over all slots; combiner-sync = all-to-all of the bitmap's per-owner blocks; the
 //     owner ORs the P blocks it receives and claims the unvisited vertices.
-// The collectives come from the caller (gre_exchange_fn): NCCL through torch.distributed in
-// graphine_b200/partition.py, or ncclAllGather / ncclAlltoAll from C++.  Direction rule, levels
-// and PageRank values are those of the one-GPU paths.
+//   * SSSP (near-far): the pending slots below a global limit relax their out-arcs into a
+//     candidate array over all slots (sssp.cu's tile kernel, atomic min); combiner-sync =
+//     all-to-all of the offers; the owner keeps the smallest and marks improved slots pending.
+//   * CC: scatter-sync = all-gather of the labels; every owned row takes the smallest label of
+//     its neighbours and of the vertex its label names (label propagation with shortcuts).
+// The collectives come from the caller (gre_exchange_fn): the library's own NCCL communicator
+// (nccl_exchange.cpp), torch.distributed (graphine_b200/partition.py), or anything else with the
+// same all-gather / all-to-all semantics.  Direction rule, levels, distances, labels and
+// PageRank values are those of the one-GPU paths.
 //
 // Vertex layout.  Internal ids are dealt to ranks one by one in snake order: round r = v / P
 // gives ranks 0, 1, .., P-1 on even rounds and P-1, .., 1, 0 on odd ones, and vertex v becomes
