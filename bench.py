@@ -445,6 +445,12 @@ def run_ours(args, rank, world, local_rank):
         all_edges, all_e2e_edges = float(w[0]), float(w[1])
     else:
         max_ms, max_e2e, all_edges, all_e2e_edges = tot_ms, e2e_s, float(tot_edges), float(e2e_edges)
+    # the partitioned block needs every rank (its collectives); rank 0 reports it
+    if world == 1 or args.partitioned:
+        psrcs = np.random.default_rng(4242).choice(nz, size=4, replace=False).astype(np.uint32)  # same on all ranks
+        part_info = partitioned_block(G, g, psrcs, world, rank, local_rank)
+    else:
+        part_info = None
     if rank != 0:
         return 0
 
@@ -462,11 +468,6 @@ def run_ours(args, rank, world, local_rank):
                       "hbm_gbs_algorithmic": v["bytes"] / (v["ms"] * 1e-3) / 1e9 if v["ms"] else None,
                       "share": v["ms"] / tot_ms}
     extra = {}
-    if world == 1 or args.partitioned:
-        psrcs = np.random.default_rng(4242).choice(nz, size=4, replace=False).astype(np.uint32)  # same on all ranks
-        part_info = partitioned_block(G, g, psrcs, world, rank, local_rank)
-    else:
-        part_info = None
     if not args.no_batched:
         # sampled betweenness on the scale-26 graph in batches of 64 sources (one batch by
         # default, --bc-sources 1024 for the full sample), then the batched-vs-looped block
