@@ -31,6 +31,9 @@
 
 namespace gre {
 
+// defined in bfs.cu
+__global__ void k_queue_to_bits(const uint32_t* __restrict__ queue, uint64_t nq, uint32_t* __restrict__ bits);
+
 template <class T>
 static int ws_array(gre_graph g, int slot, uint64_t count, T** p) {
   void* v = nullptr;
@@ -196,6 +199,132 @@ __global__ void __launch_bounds__(kTileThreads) k_sssp_relax(const uint32_t* __r
     }
     __syncthreads();
   }
+}
+
+// Large frontiers relaxed through the degree bins of the CSR instead of arc tiles: every bin's
+// rows are scanned in order, and a row whose vertex is in the frontier bitmap relaxes its light
+// ([off, lend)) or heavy ([lend, off+1)) arcs with 1..32 lanes (bins 0-5), a CTA (bin 6) or a CTA
+// per 65536-arc chunk (bin 7).  No queue scan, no tile staging and no block barriers: the
+// relaxations of a large frontier stream like the PageRank pull.  Same improvements (atomic min
+// and a changed bit) as the tile kernel.
+struct RelaxRange {
+  const uint32_t* __restrict__ front;  // frontier bitmap
+  const uint64_t* __restrict__ off;
+  const uint64_t* __restrict__ lend;
+  const uint32_t* __restrict__ col;
+  const uint32_t* __restrict__ w;
+  uint32_t* __restrict__ dist;
+  uint32_t* __restrict__ changed;
+  unsigned long long* __restrict__ arcs;  // arcs relaxed (statistics)
+  bool heavy;
+  __device__ __forceinline__ bool in(uint32_t v) const { return (__ldg(front + (v >> 5)) >> (v & 31u)) & 1u; }
+  __device__ __forceinline__ void range(uint32_t v, uint64_t* lo, uint64_t* hi) const {
+    *lo = heavy ? lend[v] : off[v];
+    *hi = heavy ? off[v + 1] : lend[v];
+  }
+  // arcs a, a + step, ... < hi offered du + w; four column/weight loads, then four distance
+  // probes in flight per lane
+  __device__ __forceinline__ void relax(uint32_t du, uint64_t a, uint64_t hi, uint64_t step) const {
+    for (; a + 3 * step < hi; a += 4 * step) {
+      uint32_t x[4], nd[4], dv[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        x[k] = __ldg(col + a + k * step);
+        nd[k] = du + __ldg(w + a + k * step);
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) dv[k] = __ldcg(dist + x[k]);
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (nd[k] < dv[k]) {
+          atomicMin(dist + x[k], nd[k]);
+          atomicOr(changed + (x[k] >> 5), 1u << (x[k] & 31u));
+        }
+    }
+    for (; a < hi; a += step) {
+      const uint32_t x = __ldg(col + a);
+      const uint32_t nd = du + __ldg(w + a);
+      if (nd < __ldcg(dist + x)) {
+        atomicMin(dist + x, nd);
+        atomicOr(changed + (x >> 5), 1u << (x & 31u));
+      }
+    }
+  }
+};
+
+__device__ __forceinline__ void add_arcs(unsigned long long* c, unsigned long long k) {
+  for (int o = 16; o > 0; o >>= 1) k += __shfl_xor_sync(0xffffffffu, k, o);
+  if ((threadIdx.x & 31u) == 0 && k) atomicAdd(c, k);
+}
+
+template <int G>
+__global__ void __launch_bounds__(256) k_relax_lanes(const uint32_t* __restrict__ rows, uint64_t count, RelaxRange R) {
+  const uint32_t lane = threadIdx.x & 31u, lig = lane % G;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned long long arcs = 0;
+  for (uint64_t base = warp * (32 / G); base < count; base += nwarps * (32 / G)) {
+    const uint64_t i = base + lane / G;
+    if (i >= count) continue;
+    const uint32_t v = rows[i];
+    if (!R.in(v)) continue;
+    uint64_t lo, hi;
+    R.range(v, &lo, &hi);
+    if (lo >= hi) continue;
+    if (lig == 0) arcs += hi - lo;
+    R.relax(__ldcg(R.dist + v), lo + lig, hi, G);
+  }
+  add_arcs(R.arcs, arcs);
+}
+
+__global__ void __launch_bounds__(256) k_relax_cta(const uint32_t* __restrict__ rows, uint64_t count, RelaxRange R) {
+  unsigned long long arcs = 0;
+  for (uint64_t i = blockIdx.x; i < count; i += gridDim.x) {
+    const uint32_t v = rows[i];
+    if (!R.in(v)) continue;
+    uint64_t lo, hi;
+    R.range(v, &lo, &hi);
+    if (threadIdx.x == 0 && hi > lo) arcs += hi - lo;
+    R.relax(__ldcg(R.dist + v), lo + threadIdx.x, hi, blockDim.x);
+  }
+  add_arcs(R.arcs, arcs);
+}
+
+// chunk c: arcs [chunk_begin[c], + chunk) of the row, cut to the light or heavy range
+__global__ void __launch_bounds__(256) k_relax_chunks(const uint32_t* __restrict__ rows, const uint64_t* __restrict__ chunk_row,
+                                                      const uint64_t* __restrict__ chunk_begin, uint64_t nchunks, uint64_t chunk,
+                                                      RelaxRange R) {
+  unsigned long long arcs = 0;
+  for (uint64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    const uint32_t v = rows[chunk_row[c]];
+    if (!R.in(v)) continue;
+    uint64_t lo, hi;
+    R.range(v, &lo, &hi);
+    const uint64_t c0 = chunk_begin[c], c1 = c0 + chunk;
+    lo = lo > c0 ? lo : c0;
+    hi = hi < c1 ? hi : c1;
+    if (lo >= hi) continue;
+    if (threadIdx.x == 0) arcs += hi - lo;
+    R.relax(__ldcg(R.dist + v), lo + threadIdx.x, hi, blockDim.x);
+  }
+  add_arcs(R.arcs, arcs);
+}
+
+static int relax_binned(const DegreeBins& B, const RelaxRange& R, cudaStream_t s) {
+  const uint32_t* r = B.rows;
+  auto grid = [](uint64_t threads) { return grid_for(threads, 256, 8); };
+  if (B.count[0]) k_relax_lanes<1><<<grid(B.count[0]), 256, 0, s>>>(r + B.start[0], B.count[0], R);
+  if (B.count[1]) k_relax_lanes<2><<<grid(B.count[1] * 2), 256, 0, s>>>(r + B.start[1], B.count[1], R);
+  if (B.count[2]) k_relax_lanes<4><<<grid(B.count[2] * 4), 256, 0, s>>>(r + B.start[2], B.count[2], R);
+  if (B.count[3]) k_relax_lanes<8><<<grid(B.count[3] * 8), 256, 0, s>>>(r + B.start[3], B.count[3], R);
+  if (B.count[4]) k_relax_lanes<16><<<grid(B.count[4] * 16), 256, 0, s>>>(r + B.start[4], B.count[4], R);
+  if (B.count[5]) k_relax_lanes<32><<<grid(B.count[5] * 32), 256, 0, s>>>(r + B.start[5], B.count[5], R);
+  if (B.count[6]) k_relax_cta<<<grid(B.count[6] * 256), 256, 0, s>>>(r + B.start[6], B.count[6], R);
+  if (B.count[7])
+    k_relax_chunks<<<grid(B.n_hub_chunks * 256), 256, 0, s>>>(r + B.start[7], B.hub_chunk_row, B.hub_chunk_begin, B.n_hub_chunks,
+                                                              B.sched.hub_chunk, R);
+  GRE_LAUNCH_CHECK();
+  return GRE_SUCCESS;
 }
 
 // Changed vertices -> next queues, one lane per bitmap word (the word is cleared).  Below the
@@ -368,6 +497,13 @@ static int relax_blocks_per_sm() {
 
 uint64_t sssp_tile_arcs() { return kTile; }
 
+// Frontiers of at least n / binned_frontier() vertices are relaxed through the degree bins
+// (default 64; the GRE_SSSP_BINNED environment variable overrides it, 0 = never).
+static uint64_t binned_frontier() {
+  if (const char* e = getenv("GRE_SSSP_BINNED")) return strtoull(e, nullptr, 10);
+  return 64;
+}
+
 // The relaxation of one frontier pass: tile starts, then k_sssp_relax over one wave of CTAs.
 int sssp_relax_tiles(cudaStream_t stream, const uint32_t* queue, uint64_t nq, const uint64_t* prefix, uint64_t total,
                      uint32_t* tstart, const uint64_t* base, const uint32_t* col, const uint32_t* w, const uint32_t* srcdist,
@@ -434,7 +570,13 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
   GRE_CHECK(ws_array(g, WS_J, nwords, &infar));
   GRE_CHECK(ws_array(g, WS_K, nwords, &inbucket));
   GRE_CHECK(ws_array(g, WS_L, n, &blist));
-  GRE_CHECK(ws_array(g, WS_COUNTERS, 8, &cnt));
+  GRE_CHECK(ws_array(g, WS_COUNTERS, 10, &cnt));  // 8 uint32 counters, then the binned passes' arc count
+  unsigned long long* binned_arcs = (unsigned long long*)(cnt + 8);
+  // large frontiers go through the degree bins of the CSR (the symmetric CSC is the CSR)
+  const bool sym = g->symmetric();
+  GRE_CHECK(ensure_bins(g, sym));
+  const DegreeBins& bins = sym ? g->bins_in : g->bins_out;
+  const uint64_t bdiv = binned_frontier();
   size_t cubbytes = 0;
   void* cubtmp = nullptr;
   cub::DeviceScan::ExclusiveSum(nullptr, cubbytes, deg, prefix, n + 1, g->stream);
@@ -443,6 +585,7 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
   GRE_CUDA(cudaMemsetAsync(changed, 0, sizeof(uint32_t) * nwords, g->stream));
   GRE_CUDA(cudaMemsetAsync(infar, 0, sizeof(uint32_t) * nwords, g->stream));
   GRE_CUDA(cudaMemsetAsync(inbucket, 0, sizeof(uint32_t) * nwords, g->stream));
+  GRE_CUDA(cudaMemsetAsync(binned_arcs, 0, sizeof(unsigned long long), g->stream));
   uint32_t limit = delta ? delta : 0xffffffffu;
   uint64_t nq = 0, nfar = 0, nb = 0, relaxed = 0, bytes = 0;
   uint32_t* q = qa;
@@ -469,6 +612,28 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
   // one relaxation pass over `list` (light or heavy ranges), the improvements classified into
   // the next near queue, the bucket list and the far pile
   auto pass = [&](const uint32_t* list, uint64_t nlist, bool heavy, uint32_t* out_near) -> int {
+    if (bdiv && nlist >= n / bdiv && nlist > 0) {
+      // the heavy pass's frontier is the bucket, already a bitmap; a light frontier is made one
+      // in the scan buffer (free in this form of the pass)
+      uint32_t* front = inbucket;
+      if (!heavy) {
+        front = (uint32_t*)deg;
+        GRE_CUDA(cudaMemsetAsync(front, 0, sizeof(uint32_t) * nwords, g->stream));
+        k_queue_to_bits<<<grid_for(nlist, 256), 256, 0, g->stream>>>(list, nlist, front);
+      }
+      GRE_CHECK(init_counters(g, cnt, 0, (uint32_t)nfar, (uint32_t)nb));
+      RelaxRange R{front, off, lend, col, w, dist, changed, binned_arcs, heavy};
+      GRE_CHECK(relax_binned(bins, R, g->stream));
+      k_sssp_classify<<<grid_for(nwords, 256, 8), 256, 0, g->stream>>>(nwords, changed, dist, off, lend, limit, out_near, infar,
+                                                                        far, inbucket, blist, cnt);
+      GRE_LAUNCH_CHECK();
+      GRE_CHECK(read_counters());
+      bytes += 4 * n + n / 8 + 8 * (uint64_t)(h[0] + h[2] - nfar + h[4] - nb);  // rows scanned, bitmap (arcs below)
+      nfar = h[2];
+      nb = h[4];
+      ++steps;
+      return GRE_SUCCESS;
+    }
     if (heavy) k_sssp_degrees<true><<<grid_for(nlist, 256), 256, 0, g->stream>>>(list, nlist, off, lend, deg);
     else k_sssp_degrees<false><<<grid_for(nlist, 256), 256, 0, g->stream>>>(list, nlist, off, lend, deg);
     GRE_CUDA(cub::DeviceScan::ExclusiveSum(cubtmp, cubbytes, deg, prefix, nlist + 1, g->stream));
@@ -538,6 +703,11 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
       std::swap(far, far2);
     }
   }
+  unsigned long long barcs = 0;
+  GRE_CUDA(cudaMemcpyAsync(&barcs, binned_arcs, sizeof barcs, cudaMemcpyDeviceToHost, g->stream));
+  GRE_CUDA(cudaStreamSynchronize(g->stream));
+  relaxed += barcs;
+  bytes += 12 * barcs;  // column + weight + distance probe per arc
   if (st) {
     st->supersteps += steps ? steps - 1 : 0;
     st->arcs_traversed += relaxed;

@@ -492,3 +492,17 @@ def test_s20_cc_properties(rmat20):
     assert np.all(lab[lab] == lab)
     lab2, _ = G.vc_cc(g)
     np.testing.assert_array_equal(lab, lab2)
+
+
+@pytest.mark.parametrize("binned", ["0", "1", "64"], ids=["tiles", "bins", "default"])
+def test_sssp_relaxation_forms_agree(monkeypatch, binned):
+    """Arc tiles only, degree bins only, and the default mix give the oracle's distances."""
+    monkeypatch.setenv("GRE_SSSP_BINNED", binned)
+    for sym in (True, False):
+        n, off, col = G.rmat_host(12, 16, 9, sym)
+        g = G.Graph.from_csr(n, off, col, dir=G.InOut if sym else G.Out, symmetric=sym, reorder=True)
+        g.set_weights_hash(3)
+        R = O.Restatement.from_csr(n, off, col)
+        roots = G.sample_sources(off, 3, 1)
+        ref = R.sssp_many(roots, 3)
+        np.testing.assert_array_equal(G.sssp(g, roots)[0].reshape(len(roots), n), ref)
