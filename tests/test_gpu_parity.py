@@ -494,7 +494,7 @@ def test_s20_cc_properties(rmat20):
     np.testing.assert_array_equal(lab, lab2)
 
 
-@pytest.mark.parametrize("binned", ["0", "1", "64"], ids=["tiles", "bins", "default"])
+@pytest.mark.parametrize("binned", ["0", "4294967296", "64"], ids=["tiles", "bins", "default"])
 def test_sssp_relaxation_forms_agree(monkeypatch, binned):
     """Arc tiles only, degree bins only, and the default mix give the oracle's distances."""
     monkeypatch.setenv("GRE_SSSP_BINNED", binned)
