@@ -50,6 +50,8 @@ enum WsSlot {
   WS_PERM_IN,    // inputs permuted to internal order
   WS_PERM_IN2,
   WS_PERM_OFF,   // caller-order row offsets
+  WS_SSSP_L,     // SSSP: vertices with light arcs (bitmap)
+  WS_SSSP_H,     // SSSP: vertices with heavy arcs (bitmap)
   WS_NSLOTS
 };
 

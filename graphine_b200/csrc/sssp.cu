@@ -327,24 +327,47 @@ static int relax_binned(const DegreeBins& B, const RelaxRange& R, cudaStream_t s
   return GRE_SUCCESS;
 }
 
+// Which vertices have light arcs ([off, lend) non-empty) and which heavy ones ([lend, off+1)):
+// one bit each, so that the passes below test a word instead of reading three offsets per vertex.
+__global__ void k_sssp_classes(uint64_t n, const uint64_t* __restrict__ off, const uint64_t* __restrict__ lend,
+                               uint32_t* __restrict__ lbits, uint32_t* __restrict__ hbits) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) & ~31ull; base < n; base += stride) {
+    const uint64_t v = base + (threadIdx.x & 31u);
+    bool light = false, heavy = false;
+    if (v < n) {
+      const uint64_t a0 = off[v], am = lend[v], a1 = off[v + 1];
+      light = am > a0;
+      heavy = a1 > am;
+    }
+    const uint32_t lw = __ballot_sync(0xffffffffu, light), hw = __ballot_sync(0xffffffffu, heavy);
+    if ((threadIdx.x & 31u) == 0) {
+      lbits[base >> 5] = lw;
+      hbits[base >> 5] = hw;
+    }
+  }
+}
+
 // Changed vertices -> next queues, one lane per bitmap word (the word is cleared).  Below the
 // limit a vertex joins the near queue if it has light arcs, and the bucket list (once per
 // bucket) if it has heavy arcs; its far entry, if any, becomes void.  At or above the limit it
 // joins the far pile unless already there.  Vertices without out-arcs are dropped.
 __global__ void k_sssp_classify(uint64_t nwords, uint32_t* __restrict__ changed, const uint32_t* __restrict__ dist,
-                                const uint64_t* __restrict__ off, const uint64_t* __restrict__ lend, uint32_t near_limit,
+                                const uint32_t* __restrict__ lbits, const uint32_t* __restrict__ hbits, uint32_t near_limit,
                                 uint32_t* __restrict__ near, uint32_t* __restrict__ infar, uint32_t* __restrict__ far,
                                 uint32_t* __restrict__ inbucket, uint32_t* __restrict__ blist, uint32_t* __restrict__ counters) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t base = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) & ~31ull; base < nwords; base += stride) {
     const uint64_t wi = base + (threadIdx.x & 31u);
-    uint32_t bits = 0, fbits = 0, bbits = 0;
+    uint32_t bits = 0, fbits = 0, bbits = 0, lw = 0, hw = 0;
     if (wi < nwords) {
       bits = changed[wi];
       if (bits) {
         changed[wi] = 0;
         fbits = infar[wi];
         bbits = inbucket[wi];
+        lw = lbits[wi];
+        hw = hbits[wi];
       }
     }
     uint32_t set_far = 0, clear_far = 0, set_bucket = 0;
@@ -355,11 +378,11 @@ __global__ void k_sssp_classify(uint64_t nwords, uint32_t* __restrict__ changed,
         const uint32_t b = __ffs(bits) - 1;
         bits &= bits - 1;
         v = (uint32_t)(wi << 5) + b;
-        const uint64_t a0 = off[v], am = lend[v], a1 = off[v + 1];
-        if (a1 > a0) {
+        const bool light = (lw >> b) & 1u, heavy = (hw >> b) & 1u;
+        if (light || heavy) {
           if (dist[v] < near_limit) {
-            to_near = am > a0;
-            if (a1 > am && !(bbits & (1u << b))) {
+            to_near = light;
+            if (heavy && !(bbits & (1u << b))) {
               to_bucket = true;
               set_bucket |= 1u << b;
             }
@@ -408,7 +431,7 @@ __global__ void k_sssp_seed(uint32_t src, const uint64_t* __restrict__ off, cons
 // entries whose far bit was cleared (the vertex went to the near queue since) are dropped.
 // counters[3] gets the smallest distance left.
 __global__ void k_far_split(const uint32_t* __restrict__ far, uint64_t nfar, const uint32_t* __restrict__ dist, uint32_t near_limit,
-                            const uint64_t* __restrict__ off, const uint64_t* __restrict__ lend, uint32_t* __restrict__ infar,
+                            const uint32_t* __restrict__ lbits, const uint32_t* __restrict__ hbits, uint32_t* __restrict__ infar,
                             uint32_t* __restrict__ near, uint32_t* __restrict__ far_out, uint32_t* __restrict__ inbucket,
                             uint32_t* __restrict__ blist, uint32_t* __restrict__ counters) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -424,9 +447,8 @@ __global__ void k_far_split(const uint32_t* __restrict__ far, uint64_t nfar, con
         const uint32_t d = dist[v];
         if (d < near_limit) {
           atomicAnd(infar + (v >> 5), ~bit);
-          const uint64_t a0 = off[v], am = lend[v], a1 = off[v + 1];
-          to_near = am > a0;
-          if (a1 > am) to_bucket = !(atomicOr(inbucket + (v >> 5), bit) & bit);
+          to_near = (lbits[v >> 5] & bit) != 0;
+          if (hbits[v >> 5] & bit) to_bucket = !(atomicOr(inbucket + (v >> 5), bit) & bit);
         } else {
           keep = true;
           dmin = min(dmin, d);
@@ -570,6 +592,9 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
   GRE_CHECK(ws_array(g, WS_J, nwords, &infar));
   GRE_CHECK(ws_array(g, WS_K, nwords, &inbucket));
   GRE_CHECK(ws_array(g, WS_L, n, &blist));
+  uint32_t *lbits, *hbits;
+  GRE_CHECK(ws_array(g, WS_SSSP_L, nwords, &lbits));
+  GRE_CHECK(ws_array(g, WS_SSSP_H, nwords, &hbits));
   GRE_CHECK(ws_array(g, WS_COUNTERS, 10, &cnt));  // 8 uint32 counters, then the binned passes' arc count
   unsigned long long* binned_arcs = (unsigned long long*)(cnt + 8);
   // large frontiers go through the degree bins of the CSR (the symmetric CSC is the CSR)
@@ -586,6 +611,7 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
   GRE_CUDA(cudaMemsetAsync(infar, 0, sizeof(uint32_t) * nwords, g->stream));
   GRE_CUDA(cudaMemsetAsync(inbucket, 0, sizeof(uint32_t) * nwords, g->stream));
   GRE_CUDA(cudaMemsetAsync(binned_arcs, 0, sizeof(unsigned long long), g->stream));
+  k_sssp_classes<<<grid_for(n, 256, 8), 256, 0, g->stream>>>(n, off, lend, lbits, hbits);
   uint32_t limit = delta ? delta : 0xffffffffu;
   uint64_t nq = 0, nfar = 0, nb = 0, relaxed = 0, bytes = 0;
   uint32_t* q = qa;
@@ -624,7 +650,7 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
       GRE_CHECK(init_counters(g, cnt, 0, (uint32_t)nfar, (uint32_t)nb));
       RelaxRange R{front, off, lend, col, w, dist, changed, binned_arcs, heavy};
       GRE_CHECK(relax_binned(bins, R, g->stream));
-      k_sssp_classify<<<grid_for(nwords, 256, 8), 256, 0, g->stream>>>(nwords, changed, dist, off, lend, limit, out_near, infar,
+      k_sssp_classify<<<grid_for(nwords, 256, 8), 256, 0, g->stream>>>(nwords, changed, dist, lbits, hbits, limit, out_near, infar,
                                                                         far, inbucket, blist, cnt);
       GRE_LAUNCH_CHECK();
       GRE_CHECK(read_counters());
@@ -644,7 +670,7 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
     if (total) {
       GRE_CHECK(sssp_relax_tiles(g->stream, list, nlist, prefix, total, tstart, heavy ? lend : off, col, w, dist, dist, changed,
                                  cnt + 1));
-      k_sssp_classify<<<grid_for(nwords, 256, 8), 256, 0, g->stream>>>(nwords, changed, dist, off, lend, limit, out_near, infar,
+      k_sssp_classify<<<grid_for(nwords, 256, 8), 256, 0, g->stream>>>(nwords, changed, dist, lbits, hbits, limit, out_near, infar,
                                                                         far, inbucket, blist, cnt);
     }
     GRE_LAUNCH_CHECK();
@@ -691,7 +717,7 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
       if (p == 0) limit = limit > 0xffffffffu - delta ? 0xffffffffu : limit + delta;
       else limit = lowest > 0xffffffffu - delta ? 0xffffffffu : lowest + delta;
       GRE_CHECK(init_counters(g, cnt, 0, 0, 0));
-      k_far_split<<<grid_for(nfar, 256, 8), 256, 0, g->stream>>>(far, nfar, dist, limit, off, lend, infar, q, far2, inbucket,
+      k_far_split<<<grid_for(nfar, 256, 8), 256, 0, g->stream>>>(far, nfar, dist, limit, lbits, hbits, infar, q, far2, inbucket,
                                                                   blist, cnt);
       GRE_LAUNCH_CHECK();
       GRE_CHECK(read_counters());
