@@ -343,6 +343,12 @@ int sssp_delta(gre_graph g, uint32_t* delta);
 // improved head; otherwise dist is a separate offer array and changed is unused.  tstart holds
 // ceil(total / sssp_tile_arcs()) entries; error is set if a tile holds too many owners.
 uint64_t sssp_tile_arcs();
+// The binned form of a relaxation pass as offers (sssp.cu): every row of the bins whose bit is set
+// in `front` offers srcdist[row] + w over all its arcs [off[row], off[row+1]) into `offers`
+// (atomic min); `arcs` counts the arcs.
+int sssp_relax_binned_offer(cudaStream_t stream, const DegreeBins& B, const uint32_t* front, const uint64_t* off,
+                            const uint32_t* col, const uint32_t* w, const uint32_t* srcdist, uint32_t* offers,
+                            unsigned long long* arcs);
 int sssp_relax_tiles(cudaStream_t stream, const uint32_t* queue, uint64_t nq, const uint64_t* prefix, uint64_t total,
                      uint32_t* tstart, const uint64_t* base, const uint32_t* col, const uint32_t* w, const uint32_t* srcdist,
                      uint32_t* dist, uint32_t* changed, uint32_t* error);

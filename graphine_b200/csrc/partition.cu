@@ -804,6 +804,7 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
   GRE_CHECK(ws_array(s, WS_OUTBUF2, P, &call));
   bc = (BfsCounters*)(c + 1);
   err = (uint32_t*)(c + 2);
+  unsigned long long* arcs_seen = (unsigned long long*)(c + 2) + 1;  // arcs of binned passes (unused: the select counts them)
   bcall = (BfsCounters*)call;
   GRE_CHECK(prepare_output(s, dist, n, WS_OUTBUF, &dout));
   void* cubtmp = nullptr;
@@ -855,7 +856,16 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
     const uint64_t nq = h[me].near;
     GRE_CUDA(cudaMemsetAsync(cand, 0xff, sizeof(uint32_t) * P * L, s->stream));
     unsigned long long total = h[me].arcs;
-    if (nq && total) {  // the one-GPU path's tile relaxation: offers go to cand, owners' distances from dl
+    if (nq && total && nq >= L / 64) {
+      // a large frontier: the one-GPU path's binned relaxation over this rank's degree bins,
+      // the queued slots as a bitmap (in the scan buffer, unused by this form)
+      uint32_t* front = (uint32_t*)deg;
+      GRE_CUDA(cudaMemsetAsync(front, 0, sizeof(uint32_t) * W, s->stream));
+      k_queue_to_bits<<<grid_for(nq, 256), 256, 0, s->stream>>>(queue, nq, front);
+      GRE_LAUNCH_CHECK();
+      const DegreeBins& B = s->roff == s->off ? s->bins_in : s->bins_out;
+      GRE_CHECK(sssp_relax_binned_offer(s->stream, B, front, s->off, s->col, p->w32, dl, cand, arcs_seen));
+    } else if (nq && total) {  // the one-GPU path's tile relaxation: offers go to cand, owners' distances from dl
       k_frontier_degrees<<<grid_for(nq, 256), 256, 0, s->stream>>>(queue, nq, s->off, deg);
       GRE_CUDA(cub::DeviceScan::ExclusiveSum(cubtmp, cubbytes, deg, prefix, nq + 1, s->stream));
       GRE_CHECK(sssp_relax_tiles(s->stream, queue, nq, prefix, total, tstart, s->off, s->col, p->w32, dl, cand, nullptr, err));

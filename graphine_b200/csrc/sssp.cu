@@ -217,13 +217,17 @@ struct RelaxRange {
   uint32_t* __restrict__ changed;
   unsigned long long* __restrict__ arcs;  // arcs relaxed (statistics)
   bool heavy;
+  const uint32_t* __restrict__ srcdist;  // OFFER form: the rows' own distances (dist holds offers)
   __device__ __forceinline__ bool in(uint32_t v) const { return (__ldg(front + (v >> 5)) >> (v & 31u)) & 1u; }
   __device__ __forceinline__ void range(uint32_t v, uint64_t* lo, uint64_t* hi) const {
     *lo = heavy ? lend[v] : off[v];
     *hi = heavy ? off[v + 1] : lend[v];
   }
   // arcs a, a + step, ... < hi offered du + w; four column/weight loads, then four distance
-  // probes in flight per lane
+  // probes in flight per lane.  OFFER: dist is a separate offer array and no changed bit is set.
+  template <bool OFFER>
+  __device__ __forceinline__ uint32_t own(uint32_t v) const { return __ldcg((OFFER ? srcdist : dist) + v); }
+  template <bool OFFER>
   __device__ __forceinline__ void relax(uint32_t du, uint64_t a, uint64_t hi, uint64_t step) const {
     for (; a + 3 * step < hi; a += 4 * step) {
       uint32_t x[4], nd[4], dv[4];
@@ -238,7 +242,7 @@ struct RelaxRange {
       for (int k = 0; k < 4; ++k)
         if (nd[k] < dv[k]) {
           atomicMin(dist + x[k], nd[k]);
-          atomicOr(changed + (x[k] >> 5), 1u << (x[k] & 31u));
+          if (!OFFER) atomicOr(changed + (x[k] >> 5), 1u << (x[k] & 31u));
         }
     }
     for (; a < hi; a += step) {
@@ -246,7 +250,7 @@ struct RelaxRange {
       const uint32_t nd = du + __ldg(w + a);
       if (nd < __ldcg(dist + x)) {
         atomicMin(dist + x, nd);
-        atomicOr(changed + (x >> 5), 1u << (x & 31u));
+        if (!OFFER) atomicOr(changed + (x >> 5), 1u << (x & 31u));
       }
     }
   }
@@ -257,7 +261,7 @@ __device__ __forceinline__ void add_arcs(unsigned long long* c, unsigned long lo
   if ((threadIdx.x & 31u) == 0 && k) atomicAdd(c, k);
 }
 
-template <int G>
+template <int G, bool OFFER>
 __global__ void __launch_bounds__(256) k_relax_lanes(const uint32_t* __restrict__ rows, uint64_t count, RelaxRange R) {
   const uint32_t lane = threadIdx.x & 31u, lig = lane % G;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
@@ -272,11 +276,12 @@ __global__ void __launch_bounds__(256) k_relax_lanes(const uint32_t* __restrict_
     R.range(v, &lo, &hi);
     if (lo >= hi) continue;
     if (lig == 0) arcs += hi - lo;
-    R.relax(__ldcg(R.dist + v), lo + lig, hi, G);
+    R.template relax<OFFER>(R.template own<OFFER>(v), lo + lig, hi, G);
   }
   add_arcs(R.arcs, arcs);
 }
 
+template <bool OFFER>
 __global__ void __launch_bounds__(256) k_relax_cta(const uint32_t* __restrict__ rows, uint64_t count, RelaxRange R) {
   unsigned long long arcs = 0;
   for (uint64_t i = blockIdx.x; i < count; i += gridDim.x) {
@@ -285,12 +290,13 @@ __global__ void __launch_bounds__(256) k_relax_cta(const uint32_t* __restrict__ 
     uint64_t lo, hi;
     R.range(v, &lo, &hi);
     if (threadIdx.x == 0 && hi > lo) arcs += hi - lo;
-    R.relax(__ldcg(R.dist + v), lo + threadIdx.x, hi, blockDim.x);
+    R.template relax<OFFER>(R.template own<OFFER>(v), lo + threadIdx.x, hi, blockDim.x);
   }
   add_arcs(R.arcs, arcs);
 }
 
 // chunk c: arcs [chunk_begin[c], + chunk) of the row, cut to the light or heavy range
+template <bool OFFER>
 __global__ void __launch_bounds__(256) k_relax_chunks(const uint32_t* __restrict__ rows, const uint64_t* __restrict__ chunk_row,
                                                       const uint64_t* __restrict__ chunk_begin, uint64_t nchunks, uint64_t chunk,
                                                       RelaxRange R) {
@@ -305,24 +311,25 @@ __global__ void __launch_bounds__(256) k_relax_chunks(const uint32_t* __restrict
     hi = hi < c1 ? hi : c1;
     if (lo >= hi) continue;
     if (threadIdx.x == 0) arcs += hi - lo;
-    R.relax(__ldcg(R.dist + v), lo + threadIdx.x, hi, blockDim.x);
+    R.template relax<OFFER>(R.template own<OFFER>(v), lo + threadIdx.x, hi, blockDim.x);
   }
   add_arcs(R.arcs, arcs);
 }
 
+template <bool OFFER>
 static int relax_binned(const DegreeBins& B, const RelaxRange& R, cudaStream_t s) {
   const uint32_t* r = B.rows;
   auto grid = [](uint64_t threads) { return grid_for(threads, 256, 8); };
-  if (B.count[0]) k_relax_lanes<1><<<grid(B.count[0]), 256, 0, s>>>(r + B.start[0], B.count[0], R);
-  if (B.count[1]) k_relax_lanes<2><<<grid(B.count[1] * 2), 256, 0, s>>>(r + B.start[1], B.count[1], R);
-  if (B.count[2]) k_relax_lanes<4><<<grid(B.count[2] * 4), 256, 0, s>>>(r + B.start[2], B.count[2], R);
-  if (B.count[3]) k_relax_lanes<8><<<grid(B.count[3] * 8), 256, 0, s>>>(r + B.start[3], B.count[3], R);
-  if (B.count[4]) k_relax_lanes<16><<<grid(B.count[4] * 16), 256, 0, s>>>(r + B.start[4], B.count[4], R);
-  if (B.count[5]) k_relax_lanes<32><<<grid(B.count[5] * 32), 256, 0, s>>>(r + B.start[5], B.count[5], R);
-  if (B.count[6]) k_relax_cta<<<grid(B.count[6] * 256), 256, 0, s>>>(r + B.start[6], B.count[6], R);
+  if (B.count[0]) k_relax_lanes<1, OFFER><<<grid(B.count[0]), 256, 0, s>>>(r + B.start[0], B.count[0], R);
+  if (B.count[1]) k_relax_lanes<2, OFFER><<<grid(B.count[1] * 2), 256, 0, s>>>(r + B.start[1], B.count[1], R);
+  if (B.count[2]) k_relax_lanes<4, OFFER><<<grid(B.count[2] * 4), 256, 0, s>>>(r + B.start[2], B.count[2], R);
+  if (B.count[3]) k_relax_lanes<8, OFFER><<<grid(B.count[3] * 8), 256, 0, s>>>(r + B.start[3], B.count[3], R);
+  if (B.count[4]) k_relax_lanes<16, OFFER><<<grid(B.count[4] * 16), 256, 0, s>>>(r + B.start[4], B.count[4], R);
+  if (B.count[5]) k_relax_lanes<32, OFFER><<<grid(B.count[5] * 32), 256, 0, s>>>(r + B.start[5], B.count[5], R);
+  if (B.count[6]) k_relax_cta<OFFER><<<grid(B.count[6] * 256), 256, 0, s>>>(r + B.start[6], B.count[6], R);
   if (B.count[7])
-    k_relax_chunks<<<grid(B.n_hub_chunks * 256), 256, 0, s>>>(r + B.start[7], B.hub_chunk_row, B.hub_chunk_begin, B.n_hub_chunks,
-                                                              B.sched.hub_chunk, R);
+    k_relax_chunks<OFFER><<<grid(B.n_hub_chunks * 256), 256, 0, s>>>(r + B.start[7], B.hub_chunk_row, B.hub_chunk_begin,
+                                                                     B.n_hub_chunks, B.sched.hub_chunk, R);
   GRE_LAUNCH_CHECK();
   return GRE_SUCCESS;
 }
@@ -346,6 +353,13 @@ __global__ void k_sssp_classes(uint64_t n, const uint64_t* __restrict__ off, con
       hbits[base >> 5] = hw;
     }
   }
+}
+
+int sssp_relax_binned_offer(cudaStream_t stream, const DegreeBins& B, const uint32_t* front, const uint64_t* off,
+                            const uint32_t* col, const uint32_t* w, const uint32_t* srcdist, uint32_t* offers,
+                            unsigned long long* arcs) {
+  RelaxRange R{front, off, off + 1, col, w, offers, nullptr, arcs, false, srcdist};
+  return relax_binned<true>(B, R, stream);
 }
 
 // Changed vertices -> next queues, one lane per bitmap word (the word is cleared).  Below the
@@ -648,8 +662,8 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
         k_queue_to_bits<<<grid_for(nlist, 256), 256, 0, g->stream>>>(list, nlist, front);
       }
       GRE_CHECK(init_counters(g, cnt, 0, (uint32_t)nfar, (uint32_t)nb));
-      RelaxRange R{front, off, lend, col, w, dist, changed, binned_arcs, heavy};
-      GRE_CHECK(relax_binned(bins, R, g->stream));
+      RelaxRange R{front, off, lend, col, w, dist, changed, binned_arcs, heavy, nullptr};
+      GRE_CHECK(relax_binned<false>(bins, R, g->stream));
       k_sssp_classify<<<grid_for(nwords, 256, 8), 256, 0, g->stream>>>(nwords, changed, dist, lbits, hbits, limit, out_near, infar,
                                                                         far, inbucket, blist, cnt);
       GRE_LAUNCH_CHECK();
