@@ -21,7 +21,16 @@ against its forward, plus one 64-source BC batch on the scale-26 graph.  `partit
 ranks, NCCL exchanges; at one GPU a one-rank communicator, checked equal to the one-GPU calls.
 
 --impl reference runs the reference GRE engine (compiled from its headers into oracle/_ref/)
-on the host CPU over a bounded sample (RMAT scale 16, same plain suite) and prints the same line.
+on the host CPU, each step the same plain suite on a bounded sample of the workload (RMAT scale
+--ref-scale, default 18, same generator and seeds; inputs from the oracle's host generator, no
+product code loaded), and prints the same line with the same `config`.  Our arm reports the
+suite on that sample graph too (`same_scale_as_reference`) and on the reference's stated
+configs (`configs`: PageRank-20 on directed RMAT-16, BFS/SSSP/CC on RMAT-22 from 16 sources),
+which `--impl reference --configs` runs on the CPU.
+
+`--gpus N` without a launcher starts N ranks itself (torch.distributed.run, one per GPU);
+under a launcher (WORLD_SIZE set) each process is one rank.  `--dry-run` exercises the rank
+plumbing on the host with gloo.
 """
 from __future__ import annotations
 
@@ -29,6 +38,8 @@ import argparse
 import json
 import os
 import re
+import shutil
+import socket
 import statistics
 import subprocess
 import sys
@@ -46,7 +57,7 @@ SEED = 26
 WSEED = 20240601
 PR_ITERS = 20
 BC_SOURCES = 64
-CPU_SCALE = 16
+REF_SCALE = 18  # scale of the reference arm's bounded sample
 
 
 def env_int(name, default):
@@ -147,68 +158,150 @@ def profiled_traffic():
 
 
 # ----------------------------------------------------------------------------------------------
-# reference arm / CPU baseline: the reference engine on the host
+# the workload's identity: one config for both arms (the reference arm times a bounded sample
+# of it and says which in cpu_baseline.sample)
 # ----------------------------------------------------------------------------------------------
-def reference_suite(scale: int, reps: int, workdir: str):
-    """Runs the reference suite `reps` times on RMAT-`scale`; returns per-rep (edges, seconds)."""
+def workload_config(scale: int, gpus: int) -> dict:
+    return {"workload": f"GRE plain suite on RMAT scale {scale} EF16 symmetric: PageRank-{PR_ITERS} (power "
+                        f"iteration, FP64), DO-BFS 1 src, SSSP 1 src (u32 w in [1,255]), CC",
+            "scale": scale, "edgefactor": 16, "graph_seed": SEED, "weight_seed": WSEED,
+            "parallelism": f"replica x{gpus}", "l2": "inputs larger than L2 (graph > 126 MB)"}
+
+
+# ----------------------------------------------------------------------------------------------
+# reference arm / CPU baseline: the reference engine on the host (no product code loaded)
+# ----------------------------------------------------------------------------------------------
+def host_info() -> dict:
+    """What the CPU numbers ran on: logical CPUs, the ones this process may use, model, sockets."""
+    info = {"nproc": os.cpu_count(), "usable_cpus": len(os.sched_getaffinity(0)), "model": None, "sockets": None,
+            "cores_per_socket": None, "threads_per_core": None}
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=20).stdout
+        keys = {"Model name": "model", "Socket(s)": "sockets", "Core(s) per socket": "cores_per_socket",
+                "Thread(s) per core": "threads_per_core"}
+        for line in out.splitlines():
+            k, _, v = line.partition(":")
+            if k.strip() in keys and info[keys[k.strip()]] is None:
+                v = v.strip()
+                info[keys[k.strip()]] = int(v) if v.isdigit() else v
+    except Exception:
+        pass
+    info["mpirun"] = shutil.which("mpirun") or None
+    return info
+
+
+def reference_suite(scale: int, reps: int, workdir: str, only=("pagerank", "bfs", "sssp", "cc")):
+    """Runs the reference suite `reps` times on RMAT-`scale` (symmetric); returns per-rep
+    (edges, seconds) and the graph's size.  Inputs come from the oracle's own generator and the
+    Graph500 numerators from the reference's own BFS levels."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import graphine_b200.gre as G
     import oracle as O
 
-    n, off, col = G.rmat_host(scale, 16, SEED, True)
+    n, off, col = O.rmat(scale, 16, SEED, True)
     prefix = os.path.join(workdir, f"rmat{scale}")
-    G.write_edgelists(prefix, n, off, col, 4)
-    roots = G.sample_sources(off, reps, 5)
-    G.write_roots(prefix, roots)
-    R = O.Restatement.from_csr(n, off, col)
+    O.write_edgelists(prefix, n, off, col, 4)
+    roots = O.sample_sources(off, reps, 5)
+    O.write_roots(prefix, roots)
     m_arcs = len(col)
     m_und = m_arcs // 2
-    # reached-component edge counts (Graph500 numerator) from the oracle's levels
-    deg = np.diff(off.astype(np.int64))
-    lv = R.bfs_many(roots)
-    comp_edges = [int(deg[lv[i] >= 0].sum() // 2) for i in range(len(roots))]
-    t = {}
-    _, run = O.run_reference("pagerank", prefix, "iter", PR_ITERS, reps)
-    t["pagerank"] = run.seconds
-    _, run = O.run_reference("bfs", prefix, reps)  # the first `reps` roots
-    t["bfs"] = run.seconds[0::2]  # runs alternate: BFS plugin, Forward levels
-    _, run = O.run_reference("sssp", prefix, WSEED, reps)
-    t["sssp"] = run.seconds
-    _, run = O.run_reference("cc", prefix, reps)
-    t["cc"] = run.seconds
-    out = []
+    t = {k: [0.0] * reps for k in ("pagerank", "bfs", "sssp", "cc")}
+    comp = [0] * reps
+    if "pagerank" in only:
+        _, run = O.run_reference("pagerank", prefix, "iter", PR_ITERS, reps, timeout=7200)
+        t["pagerank"] = run.seconds
+    if "bfs" in only or "sssp" in only:
+        lv, run = O.run_reference("bfs", prefix, reps, timeout=7200)  # the first `reps` roots
+        comp = [O.reached_edges(off, lv[i * n:(i + 1) * n]) for i in range(reps)]
+        if "bfs" in only:
+            t["bfs"] = run.seconds[0::2]  # runs alternate: the BFS plugin, then the Forward levels
+    if "sssp" in only:
+        _, run = O.run_reference("sssp", prefix, WSEED, reps, timeout=7200)
+        t["sssp"] = run.seconds
+    if "cc" in only:
+        _, run = O.run_reference("cc", prefix, reps, timeout=7200)
+        t["cc"] = run.seconds
+    per = {k: [(0, 0.0)] * reps for k in t}
     for r in range(reps):
-        edges = m_arcs * PR_ITERS + comp_edges[r] + comp_edges[r] + m_und
-        secs = t["pagerank"][r] + t["bfs"][r] + t["sssp"][r] + t["cc"][r]
-        out.append((edges, secs))
-    return out, {"n": n, "m": m_arcs}
+        per["pagerank"][r] = (m_arcs * PR_ITERS, t["pagerank"][r])
+        per["bfs"][r] = (comp[r], t["bfs"][r])
+        per["sssp"][r] = (comp[r], t["sssp"][r])
+        per["cc"][r] = (m_und, t["cc"][r])
+    out = [(sum(per[k][r][0] for k in only), sum(per[k][r][1] for k in only)) for r in range(reps)]
+    return out, {"n": n, "m": m_arcs, "per": per}
 
 
-def cpu_cores_used():
-    return 12  # the reference engine's fixed worker pool (Engine.hpp:211); plus its master thread
+def reference_configs(workdir: str) -> dict:
+    """The reference on the stated configs: PageRank-20 on directed RMAT-16 (both plugins, np = 1;
+    np = 4 needs MPI), and BFS / SSSP / CC on symmetric RMAT-22 from 16 sources (harmonic mean of
+    per-source GTEPS for BFS and SSSP)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    res = {}
+    n, off, col = O.rmat(16, 16, 1, False)
+    prefix = os.path.join(workdir, "pr16")
+    O.write_edgelists(prefix, n, off, col, 4)
+    for variant in ("gre", "iter"):
+        _, run = O.run_reference("pagerank", prefix, variant, PR_ITERS, 3, timeout=3600)
+        s = statistics.median(run.seconds)
+        res[f"pagerank_{variant}_s16_dir"] = {"gteps": len(col) * PR_ITERS / s / 1e9, "seconds": s, "np": 1,
+                                              "arcs": len(col)}
+    res["pagerank_s16_dir_np4"] = "unavailable (no MPI on host)" if not shutil.which("mpirun") else         "not run (MPI present; the harness is built against the single-rank shim)"
+    n, off, col = O.rmat(22, 16, 22, True)
+    prefix = os.path.join(workdir, "s22")
+    O.write_edgelists(prefix, n, off, col, 4)
+    roots = O.sample_sources(off, 16, 22)
+    O.write_roots(prefix, roots)
+    lv, run = O.run_reference("bfs", prefix, 16, timeout=7200)
+    comp = [O.reached_edges(off, lv[i * n:(i + 1) * n]) for i in range(16)]
+    hm = lambda xs: len(xs) / sum(1.0 / x for x in xs)  # noqa: E731
+    res["bfs_s22_16src"] = {"gteps_hmean": hm([c / s / 1e9 for c, s in zip(comp, run.seconds[0::2])]),
+                            "seconds_total": sum(run.seconds[0::2])}
+    _, run = O.run_reference("sssp", prefix, WSEED, 16, timeout=7200)
+    res["sssp_s22_16src"] = {"gteps_hmean": hm([c / s / 1e9 for c, s in zip(comp, run.seconds)]),
+                             "seconds_total": sum(run.seconds)}
+    _, run = O.run_reference("cc", prefix, 1, timeout=7200)
+    res["cc_s22"] = {"gteps": (len(col) // 2) / run.seconds[0] / 1e9, "seconds": run.seconds[0]}
+    res["graph_s22"] = {"n": n, "arcs": len(col)}
+    return res
+
+
+REF_THREADS = 12  # the reference engine's fixed worker pool (Engine.hpp:211), plus its master thread
 
 
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return 0
+    t0 = time.perf_counter()
     with tempfile.TemporaryDirectory() as td:
-        res, info = reference_suite(CPU_SCALE, args.warmup + args.steps, td)
+        res, info = reference_suite(args.ref_scale, args.warmup + args.steps, td)
+        configs = reference_configs(td) if args.configs else None
     timed = res[args.warmup:]
     edges = sum(e for e, _ in timed)
     secs = sum(s for _, s in timed)
     value = edges / secs / 1e9
+    host = host_info()
+    sample = (f"each step: the plain suite on RMAT-{args.ref_scale} symmetric EF16 (n={info['n']}, arcs={info['m']}, "
+              f"same generator and seeds as the scale-{args.scale} workload; the scale-{args.scale} graph needs "
+              f"~40 B/arc of host RAM in the reference loader and hours at -O0), reference GRE engine built -O0 from "
+              f"its headers, np=1 (single-rank MPI shim), engine.run timed with MPI_Wtime as usr/test_*.cpp do; "
+              f"{REF_THREADS} engine worker threads + master on {host['usable_cpus']} usable of {host['nproc']} "
+              f"logical CPUs ({host['model']}, {host['sockets']} socket(s))")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+u32", "data": "synthetic",
-        "config": {"workload": f"GRE plain suite (PageRank-20 iter, BFS, SSSP, CC) on RMAT scale {CPU_SCALE} "
-                               f"symmetric EF16 (bounded sample of the scale-26 workload)",
-                   "graph_n": info["n"], "graph_arcs": info["m"], "parallelism": "cpu"},
-        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": cpu_cores_used(), "kind": "reference",
-                         "sample": f"RMAT-{CPU_SCALE} symmetric, reference GRE engine -O0 np=1, "
-                                   f"engine.run timed (MPI_Wtime), {args.steps} suites"},
+        "config": workload_config(args.scale, args.gpus),
+        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": REF_THREADS, "kind": "reference",
+                         "sample": sample, "host": host},
+        "per_algorithm": {k: {"gteps": sum(e for e, _ in v[args.warmup:]) / max(sum(s for _, s in v[args.warmup:]), 1e-12) / 1e9,
+                              "ms_per_step": sum(s for _, s in v[args.warmup:]) / args.steps * 1e3}
+                          for k, v in info["per"].items()},
         "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": time.perf_counter() - t0,
     }
+    if configs is not None:
+        line["configs"] = configs
     print(json.dumps(line), flush=True)
     return 0
 
@@ -216,6 +309,64 @@ def run_reference_arm(args, rank, world):
 # ----------------------------------------------------------------------------------------------
 # our arm
 # ----------------------------------------------------------------------------------------------
+def configs_block(G, dev_index: int) -> dict:
+    """The GPU on the reference's stated configs (the same graphs and sources as
+    `--impl reference --configs`): PageRank-20 on directed RMAT-16 (both plugins), and BFS / SSSP
+    / CC on symmetric RMAT-22 from 16 sources (harmonic mean of per-source GTEPS for BFS and
+    SSSP, Graph500 numerators).  Device-resident outputs, device time per call."""
+    import torch
+
+    dev = torch.device("cuda", dev_index)
+    res = {}
+    g = G.Graph.rmat(16, 16, 1, False, device=dev_index, reorder=True)
+    pr = torch.empty(g.n, dtype=torch.float64, device=dev)
+    for variant, name in ((G.PR_REFERENCE, "gre"), (G.PR_ITER, "iter")):
+        G.pagerank(g, variant, 0.85, PR_ITERS, out=pr)
+        ms = statistics.median(G.pagerank(g, variant, 0.85, PR_ITERS, out=pr)[1].device_ms for _ in range(5))
+        res[f"pagerank_{name}_s16_dir"] = {"gteps": g.m * PR_ITERS / (ms * 1e-3) / 1e9, "ms": ms, "arcs": g.m}
+    del g
+    g = G.Graph.rmat(22, 16, 22, True, device=dev_index, reorder=True)
+    g.set_weights_hash(WSEED)
+    off, _ = g.csr()
+    roots = G.sample_sources(off, 16, 22)
+    out = torch.empty(g.n, dtype=torch.int32, device=dev)
+    hm = lambda xs: len(xs) / sum(1.0 / x for x in xs)  # noqa: E731
+    for name, call in (("bfs", G.bfs), ("sssp", G.sssp)):
+        call(g, roots[:1], out=out)
+        sts = [call(g, [int(r)], out=out)[1] for r in roots]
+        res[f"{name}_s22_16src"] = {"gteps_hmean": hm([s.gteps for s in sts]),
+                                    "ms_total": sum(s.device_ms for s in sts)}
+    G.cc(g, out=out)
+    st = G.cc(g, out=out)[1]
+    res["cc_s22"] = {"gteps": st.gteps, "ms": st.device_ms}
+    res["graph_s22"] = {"n": g.n, "arcs": g.m}
+    return res
+
+
+def same_scale_block(G, dev_index: int, args) -> dict:
+    """The plain suite on the reference arm's sample graph (RMAT-`ref_scale`, same seeds and
+    sources), so that both arms can be compared on equal inputs as well."""
+    import torch
+
+    dev = torch.device("cuda", dev_index)
+    g = G.Graph.rmat(args.ref_scale, 16, SEED, True, device=dev_index, reorder=True)
+    g.set_weights_hash(WSEED)
+    off, _ = g.csr()
+    reps = args.warmup + args.steps
+    roots = G.sample_sources(off, reps, 5)
+    pr = torch.empty(g.n, dtype=torch.float64, device=dev)
+    o32 = torch.empty(g.n, dtype=torch.int32, device=dev)
+    edges, ms = 0, 0.0
+    for i, r in enumerate(roots):
+        sts = [G.pagerank(g, G.PR_ITER, 0.85, PR_ITERS, out=pr)[1], G.bfs(g, [int(r)], out=o32)[1],
+               G.sssp(g, [int(r)], out=o32)[1], G.cc(g, out=o32)[1]]
+        if i >= args.warmup:
+            edges += sum(s.traversed_edges for s in sts)
+            ms += sum(s.device_ms for s in sts)
+    return {"scale": args.ref_scale, "n": g.n, "arcs": g.m, "steps": args.steps, "gteps": edges / (ms * 1e-3) / 1e9,
+            "ms_per_step": ms / args.steps}
+
+
 def batched_block(G, dev_index: int, scale: int, seed: int):
     """Batched forms vs their looped plain forms at equal results (measured once, untimed for
     `value`): 256-source BC, 64-source BFS, 128 personalised PageRank vectors, a batch of 32
@@ -360,6 +511,43 @@ def partitioned_block(G, g, srcs, world: int, rank: int, local_rank: int) -> dic
         x.free()
 
 
+def sharded_bc_block(G, g, nz, args, world: int, local_rank: int) -> dict:
+    """Sampled betweenness on the main graph: `bc_sources` sources per rank in frontier words of
+    64, spread over the ranks by shard.bc (every rank runs the batched kernels on its own graph
+    copy, no exchange during the run) and one NCCL sum of the per-rank FP64 vectors (8n bytes).
+    Device time of each rank's batches, max over ranks; the sum's time beside it."""
+    import torch
+
+    from graphine_b200 import shard
+
+    dev = torch.device("cuda", local_rank)
+    k = args.bc_sources * world
+    srcs = np.sort(np.random.default_rng(31).choice(nz, size=k, replace=False)).astype(np.uint32)  # same on all ranks
+    mine = {"ms": 0.0, "edges": 0}
+
+    def partial(block):
+        out, st = G.bc(g, block, batched=True)
+        mine["ms"], mine["edges"] = st.device_ms, st.traversed_edges
+        return out
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    total = shard.bc(g, srcs, partial=partial)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    t = torch.tensor([mine["ms"], wall], dtype=torch.float64, device=dev)
+    e = torch.tensor([float(mine["edges"])], dtype=torch.float64, device=dev)
+    if world > 1:
+        import torch.distributed as tdist
+
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        tdist.all_reduce(e, op=tdist.ReduceOp.SUM)
+    ms, wall = float(t[0]), float(t[1])
+    return {"sources": k, "ranks": world, "ms": ms, "gteps": float(e[0]) / (ms * 1e-3) / 1e9,
+            "wall_s_with_sum": wall, "collective": "one all-reduce (sum) of n FP64" if world > 1 else "none (one rank)",
+            "checksum": float(np.sum(total))}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import graphine_b200.gre as G
@@ -451,6 +639,7 @@ def run_ours(args, rank, world, local_rank):
         part_info = partitioned_block(G, g, psrcs, world, rank, local_rank)
     else:
         part_info = None
+    bc_info = None if args.no_batched else sharded_bc_block(G, g, nz, args, world, local_rank)
     if rank != 0:
         return 0
 
@@ -469,33 +658,32 @@ def run_ours(args, rank, world, local_rank):
                       "share": v["ms"] / tot_ms}
     extra = {}
     if not args.no_batched:
-        # sampled betweenness on the scale-26 graph in batches of 64 sources (one batch by
-        # default, --bc-sources 1024 for the full sample), then the batched-vs-looped block
-        srcs = np.sort(rng.choice(nz, size=args.bc_sources, replace=False)).astype(np.uint32)
-        _, s = G.bc(g, srcs, batched=True)
-        extra[f"bc{args.bc_sources}_s26"] = {"ms": s.device_ms, "gteps": s.traversed_edges / (s.device_ms * 1e-3) / 1e9,
-                                             "sources": args.bc_sources}
+        extra[f"bc{args.bc_sources}_s{args.scale}"] = bc_info
         del g
         torch.cuda.empty_cache()
         extra.update(batched_block(G, local_rank, args.batch_scale, 77))
+    if not args.no_batched:
+        extra["configs"] = configs_block(G, local_rank)
+        extra["same_scale_as_reference"] = same_scale_block(G, local_rank, args)
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         with tempfile.TemporaryDirectory() as td:
-            res, info = reference_suite(CPU_SCALE, 1, td)
+            res, info = reference_suite(args.ref_scale, 1, td)
         e, s = res[0]
-        cpu = {"value": e / s / 1e9, "unit": "GTEPS", "cores": cpu_cores_used(), "kind": "reference",
-               "sample": f"one plain suite on RMAT-{CPU_SCALE} symmetric (n={info['n']}, arcs={info['m']}), reference "
-                         f"GRE engine -O0 np=1, engine.run timed"}
+        host = host_info()
+        cpu = {"value": e / s / 1e9, "unit": "GTEPS", "cores": REF_THREADS, "kind": "reference",
+               "sample": f"one plain suite on RMAT-{args.ref_scale} symmetric (n={info['n']}, arcs={info['m']}), "
+                         f"reference GRE engine -O0 np=1, engine.run timed; {REF_THREADS} engine worker threads + "
+                         f"master on {host['usable_cpus']} usable of {host['nproc']} logical CPUs ({host['model']}, "
+                         f"{host['sockets']} socket(s))",
+               "host": host}
     d2h = n * (8 + 4 + 4 + 4)
     line = {
         "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64+u32", "data": "synthetic",
-        "config": {"workload": f"GRE plain suite on RMAT scale {args.scale} EF16 symmetric: PageRank-{PR_ITERS} (power "
-                               f"iteration, FP64), DO-BFS 1 src, SSSP 1 src (u32 w in [1,255]), CC",
-                   "graph_n": n, "graph_arcs": m, "parallelism": f"replica x{world}",
-                   "row_schedule": sched,
-                   "l2": "inputs larger than L2 (graph > 126 MB)"},
+        "config": workload_config(args.scale, world),
+        "graph": {"n": n, "arcs": m, "relabelled": not args.no_reorder, "row_schedule": sched},
         "per_algorithm": per_alg,
         "roofline": {"bound": "hbm", "kernel": "PageRank pull superstep (degree-binned row kernels)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak if achieved else None,
@@ -512,6 +700,63 @@ def run_ours(args, rank, world, local_rank):
     return 0
 
 
+def free_port() -> int:
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
+def spawn_ranks(args) -> int:
+    """`--gpus N` without a launcher: start N ranks on this node (one per GPU) through
+    torch.distributed.run, with this command line, and return the launcher's status."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(free_port()), os.path.abspath(__file__)] + sys.argv[1:]
+    env = dict(os.environ, OMP_NUM_THREADS=os.environ.get("OMP_NUM_THREADS", "8"))
+    try:
+        return subprocess.run(cmd, env=env, timeout=args.launch_timeout).returncode
+    except subprocess.TimeoutExpired:
+        print(json.dumps({"error": f"ranks did not finish within {args.launch_timeout} s"}), flush=True)
+        return 1
+
+
+def run_dry(args, rank, world) -> int:
+    """Rank plumbing without a GPU (gloo): every rank times a small host-side step, the time is the
+    max over ranks and the work the sum, rank 0 prints the line."""
+    import torch
+    import torch.distributed as tdist
+
+    if world > 1:
+        import datetime
+
+        tdist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    try:
+        x = np.arange(1 << 16, dtype=np.float64) + rank
+        for _ in range(args.warmup):
+            float(x.sum())
+        if world > 1:
+            tdist.barrier()
+        t0 = time.perf_counter()
+        work = 0
+        for _ in range(args.steps):
+            work += int(x.size)
+            float(np.sqrt(x).sum())
+        dt = time.perf_counter() - t0
+        t = torch.tensor([dt, float(work), 1.0], dtype=torch.float64)
+        if world > 1:
+            tmax = t.clone()
+            tdist.all_reduce(tmax, op=tdist.ReduceOp.MAX)
+            tdist.all_reduce(t, op=tdist.ReduceOp.SUM)
+            t[0] = tmax[0]
+        if rank == 0:
+            print(json.dumps({"dry_run": True, "metric": METRIC, "n_gpus": world, "ranks_reporting": int(t[2]),
+                              "steps": args.steps, "warmup": args.warmup, "value": float(t[1]) / max(float(t[0]), 1e-9),
+                              "unit": "elements/s (host)", "config": workload_config(args.scale, world)}), flush=True)
+        return 0
+    finally:
+        if world > 1:
+            tdist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -519,6 +764,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=int, default=26)
+    ap.add_argument("--ref-scale", type=int, default=REF_SCALE,
+                    help="scale of the reference arm's bounded sample (and of the CPU baseline)")
+    ap.add_argument("--configs", action="store_true",
+                    help="reference arm: also run the stated configs (PageRank S16 directed, BFS/SSSP/CC S22 x 16 "
+                         "sources); minutes of CPU time")
     ap.add_argument("--batch-scale", type=int, default=20)
     ap.add_argument("--bc-sources", type=int, default=BC_SOURCES, help="sampled BC sources at the main scale")
     ap.add_argument("--no-batched", action="store_true")
@@ -527,8 +777,14 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--partitioned", action="store_true",
                     help="also run the 1D-partitioned BFS/PageRank over the ranks (always at one GPU)")
+    ap.add_argument("--dry-run", action="store_true", help="rank plumbing only, on the host (gloo), no GPU")
+    ap.add_argument("--launch-timeout", type=int, default=3600)
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ and args.impl == "ours":
+        return spawn_ranks(args)
     rank, world, local_rank = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
+    if args.dry_run:
+        return run_dry(args, rank, world)
     if args.impl == "reference":
         return run_reference_arm(args, rank, world)
     if world > 1:

@@ -189,14 +189,21 @@ static int bc_single(gre_graph g, const std::vector<uint32_t>& hs, double* dbc, 
       GRE_CHECK(ws_array(g, WS_BC4, n + 2, &hist));
       GRE_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * (n + 2), g->stream));
       k_level_hist<<<grid_for(n, 256), 256, 0, g->stream>>>(n, level, hist);
-      std::vector<uint32_t> hh(std::min<uint64_t>(n + 2, 4096));
-      GRE_CUDA(cudaMemcpyAsync(hh.data(), hist, sizeof(uint32_t) * hh.size(), cudaMemcpyDeviceToHost, g->stream));
-      GRE_CUDA(cudaStreamSynchronize(g->stream));
-      for (size_t l = 0; l < hh.size(); ++l)
-        if (hh[l]) maxl = (int32_t)l;
-      if (hh.size() < n + 2 && hh.back()) {
-        set_error("gre_bc: more than 4094 BFS levels");
-        return GRE_NOT_IMPLEMENTED;
+      // BFS levels are contiguous from 0, so the first empty bin ends them; the bins are read
+      // back in growing blocks until one holds an empty bin (one 16 KB read for most graphs)
+      std::vector<uint32_t> hh;
+      uint64_t have = 0;
+      maxl = -1;
+      while (maxl < 0 && have < n + 2) {
+        const uint64_t take = std::min<uint64_t>(n + 2 - have, std::max<uint64_t>(4096, have));
+        hh.resize(have + take);
+        GRE_CUDA(cudaMemcpyAsync(hh.data() + have, hist + have, sizeof(uint32_t) * take, cudaMemcpyDeviceToHost,
+                                 g->stream));
+        GRE_CUDA(cudaStreamSynchronize(g->stream));
+        uint64_t l = have;
+        while (l < have + take && hh[l]) ++l;
+        if (l < have + take) maxl = (int32_t)l - 1;
+        have += take;
       }
       nl = (uint32_t)maxl + 1;
       std::vector<uint32_t> start(nl + 1, 0);

@@ -321,6 +321,8 @@ inline void stats_reset(gre_stats* st) {
   st->traversed_edges = 0;
   st->algo_bytes = 0;
   st->device_ms = 0;
+  st->plugin_value = 0;
+  st->plugin_count = 0;
 }
 inline void stats_record(gre_stats* st, uint64_t active) {
   if (st && st->n_recorded < GRE_MAX_RECORDED_SUPERSTEPS) st->active[st->n_recorded++] = active;

@@ -11,8 +11,9 @@
 // The array is shared by every call on a device and keeps the last call's contents: everything
 // that must start at zero is cleared at the start of each call, and calls that overlap on the
 // GPU (two streams, two threads) race on it.  The device address of the array is looked up once
-// per device, with that device current, by the first call on it (cudaGetSymbolAddress); make that
-// first call before any stream capture.  Every GPU that loads this library's module holds the
+// per device, with that device current, by the first call on it (cudaGetSymbolAddress), and again
+// if that device's context was replaced since (cudaDeviceReset); make the first call after such
+// a change before any stream capture.  Every GPU that loads this library's module holds the
 // array until the process exits.
 //
 // It launches the kernels of the workspace-backed gre_bfs (bfs.cu) with pointers carved from the
@@ -65,19 +66,50 @@ __global__ void k_noalloc_unperm(uint64_t n, const uint32_t* __restrict__ iperm,
 
 static std::mutex g_scratch_mu;
 static void* g_scratch_addr[256];
+static void* g_scratch_ctx[256];  // the context the address was looked up in
 
-// Device address of the scratch array on `device` (looked up once per device, that device current).
+// The current context, through the driver entry point the runtime exposes (no libcuda link).
+typedef int (*CtxGetCurrentFn)(void**);
+static void* current_context() {
+  static CtxGetCurrentFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return (CtxGetCurrentFn)f;
+  }();
+  void* ctx = nullptr;
+  if (fn) fn(&ctx);
+  return ctx;
+}
+
+// Device address of the scratch array on `device` (that device current).  Looked up once per
+// device, and again only if the device's context changed since (after a cudaDeviceReset the
+// module, and with it the array, is loaded anew at another address).
 static int scratch_address(int device, unsigned char** out) {
   if (device < 0 || device >= 256) return GRE_INVALID_ARG;
   std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_addr[device]) {
+  void* ctx = current_context();
+  if (!g_scratch_addr[device] || ctx != g_scratch_ctx[device]) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return cuda_status(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
     g_scratch_addr[device] = p;
+    g_scratch_ctx[device] = ctx;
   }
   *out = (unsigned char*)g_scratch_addr[device];
   return GRE_SUCCESS;
+}
+
+// `p` is device memory that the graph's device can write: memory of that device, or managed.
+static bool on_device(const void* p, int device) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();  // clear the sticky-free error of an unregistered host pointer
+    return false;
+  }
+  return a.type == cudaMemoryTypeManaged || (a.type == cudaMemoryTypeDevice && a.device == device);
 }
 
 static uint64_t align256(uint64_t x) { return (x + 255) & ~255ull; }
@@ -101,8 +133,9 @@ int gre_bfs_noalloc(gre_graph g, uint32_t src, int32_t* level, gre_stats* st) {
     return GRE_INVALID_ARG;
   }
   GRE_CHECK(use_graph(g));
-  if (!is_device_ptr(level)) {
-    set_error("gre_bfs_noalloc: `level` must be device memory (this entry point stages nothing)");
+  if (!on_device(level, g->device)) {
+    set_error("gre_bfs_noalloc: `level` must be device memory on the graph's device %d (this entry point "
+              "stages nothing)", g->device);
     return GRE_INVALID_ARG;
   }
   unsigned char* base = nullptr;

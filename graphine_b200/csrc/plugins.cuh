@@ -8,6 +8,59 @@
 
 namespace gre {
 
+// output_statistics helpers: fixed-shape reductions, so a sum is the same bits on every run.
+namespace plugin_stats {
+constexpr int kBlocks = 256, kThreads = 256;
+// per-block sums of x[0..n) into partial[0..kBlocks), then their sum into partial[kBlocks]
+__global__ void __launch_bounds__(kThreads) k_sum_f64(const double* __restrict__ x, uint64_t n, double* __restrict__ partial) {
+  __shared__ double s[kThreads];
+  double a = 0.0;
+  for (uint64_t v = blockIdx.x * (uint64_t)kThreads + threadIdx.x; v < n; v += (uint64_t)kBlocks * kThreads) a += x[v];
+  s[threadIdx.x] = a;
+  __syncthreads();
+  for (int w = kThreads / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = s[0];
+}
+__global__ void k_sum_partials(double* partial) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double a = 0.0;
+  for (int b = 0; b < kBlocks; ++b) a += partial[b];
+  partial[kBlocks] = a;
+}
+// number of v with lab[v] == vid(v) (CC.hpp:80-94), or the sum of cnt[v] (CountIn.hpp:78-86)
+__global__ void k_count(uint64_t n, const uint32_t* __restrict__ lab, const uint32_t* __restrict__ vid,
+                        const int32_t* __restrict__ cnt, unsigned long long* __restrict__ out) {
+  unsigned long long a = 0;
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x)
+    a += lab ? (lab[v] == (vid ? vid[v] : (uint32_t)v) ? 1ull : 0ull) : (unsigned long long)cnt[v];
+  for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+  if ((threadIdx.x & 31u) == 0 && a) atomicAdd(out, a);
+}
+
+// Host side: run one reduction on the engine's stream and store it in *out_value / *out_count.
+inline void sum_f64(const EngineContext& ctx, const double* x, double* scratch, double* out_value) {
+  if (!out_value) return;
+  k_sum_f64<<<kBlocks, kThreads, 0, ctx.stream>>>(x, ctx.n, scratch);
+  k_sum_partials<<<1, 32, 0, ctx.stream>>>(scratch);
+  cudaMemcpyAsync(out_value, scratch + kBlocks, sizeof(double), cudaMemcpyDeviceToHost, ctx.stream);
+  cudaStreamSynchronize(ctx.stream);
+}
+inline void count(const EngineContext& ctx, const uint32_t* lab, const uint32_t* vid, const int32_t* cnt, double* scratch,
+                  uint64_t* out_count) {
+  if (!out_count) return;
+  unsigned long long* d = (unsigned long long*)scratch;
+  unsigned long long h = 0;
+  cudaMemsetAsync(d, 0, sizeof h, ctx.stream);
+  k_count<<<kBlocks, kThreads, 0, ctx.stream>>>(ctx.n, lab, vid, cnt, d);
+  cudaMemcpyAsync(&h, d, sizeof h, cudaMemcpyDeviceToHost, ctx.stream);
+  cudaStreamSynchronize(ctx.stream);
+  *out_count = h;
+}
+}  // namespace plugin_stats
+
 // PageRank (Kernels/PageRank.hpp:38-79).  refresh=false is the reference verbatim (pr_scatter
 // is set in init only); refresh=true is PageRankIter (pr_scatter = pr/outdeg in apply).
 struct VcPageRank {
@@ -19,6 +72,8 @@ struct VcPageRank {
   double tele;  // 0.15 in the reference (dampingFactor, PageRank.hpp:20)
   double d;     // 1 - 0.15
   bool refresh;
+  double* stat_scratch = nullptr;  // device, plugin_stats::kBlocks + 1 doubles
+  double* stat_sum = nullptr;      // host: output_statistics' sum of pr (null: not reported)
   __device__ bool init(uint32_t v) {
     pr[v] = tele;
     const uint32_t od = outdeg[v];
@@ -45,6 +100,9 @@ struct VcPageRank {
   }
   __device__ bool assert_to_halt(uint32_t) { return false; }
   void reduce() {}
+  // "Sum of pr" (PageRank.hpp:102-124; the agent and edge counts it also prints are 0 and m at
+  // one rank)
+  void output_statistics(const EngineContext& ctx) { plugin_stats::sum_f64(ctx, pr, stat_scratch, stat_sum); }
 };
 
 // BFS (Kernels/BFS.hpp:34-72): parent tree, first writer wins.  `level` (optional) records the
@@ -190,6 +248,8 @@ struct VcCountIn {
   int32_t* cn;
   int32_t* scat;
   int32_t* comb;
+  double* stat_scratch = nullptr;  // device, one 8-byte counter
+  uint64_t* stat_count = nullptr;  // host: output_statistics' "Number of in edges" (null: not reported)
   __device__ bool init(uint32_t v) {
     cn[v] = 0;
     scat[v] = 1;
@@ -207,6 +267,8 @@ struct VcCountIn {
   }
   __device__ bool assert_to_halt(uint32_t) { return true; }
   void reduce() {}
+  // "Number of in edges": the sum of the counts (CountIn.hpp:78-100)
+  void output_statistics(const EngineContext& ctx) { plugin_stats::count(ctx, nullptr, nullptr, cn, stat_scratch, stat_count); }
 };
 
 // ConnectedComponents (Kernels/CC.hpp:33-67): min-vid label propagation.  Labels are vids,
@@ -217,6 +279,8 @@ struct VcCC {
   uint32_t* scat;
   uint32_t* comb;
   const uint32_t* vid;  // get_vid: internal -> caller id, null = identity
+  double* stat_scratch = nullptr;  // device, one 8-byte counter
+  uint64_t* stat_count = nullptr;  // host: the number of components (null: not reported)
   __device__ bool init(uint32_t v) {
     cc[v] = vid ? vid[v] : v;  // cc[lv] = graph.get_vid(lv)
     scat[v] = cc[v];
@@ -237,6 +301,9 @@ struct VcCC {
   }
   __device__ bool assert_to_halt(uint32_t) { return true; }
   void reduce() {}
+  // "Number of components" (CC.hpp:73-120 prints it from reduce every superstep; the value
+  // after the last superstep is the one reported here)
+  void output_statistics(const EngineContext& ctx) { plugin_stats::count(ctx, cc, vid, nullptr, stat_scratch, stat_count); }
 };
 
 // BC Forward (Kernels/BC.hpp:56-91): level and path count; numPaths is FP64 here (the

@@ -63,7 +63,9 @@ int gre_vc_pagerank(gre_graph g, int variant, uint32_t max_supersteps, double* p
   GRE_CHECK(g->ws.get(WS_D, vc_scratch_bytes(n), &scratch));
   RunTimer timer(g);
   GRE_CUDA(cudaMemsetAsync(comb, 0, sizeof(double) * n, g->stream));  // allocCombineData(pr_combine, 0.0)
-  VcPageRank vc{dpr, scat, comb, g->outdeg, 0.15, 1.0 - 0.15, variant == GRE_PR_ITER};
+  double* stat;
+  GRE_CHECK(ws_array(g, WS_COUNTERS, plugin_stats::kBlocks + 8, &stat));
+  VcPageRank vc{dpr, scat, comb, g->outdeg, 0.15, 1.0 - 0.15, variant == GRE_PR_ITER, stat, st ? &st->plugin_value : nullptr};
   SourceSet all;
   all.all = true;
   GRE_CHECK(run_engine(g, vc, GRE_DIR_OUT, all, max_supersteps, scratch, st, nullptr, nullptr));
@@ -241,7 +243,9 @@ int gre_vc_count_in(gre_graph g, int dir, uint32_t max_supersteps, int32_t* coun
   RunTimer timer(g);
   GRE_CUDA(cudaMemsetAsync(cn, 0, sizeof(int32_t) * n, g->stream));
   GRE_CUDA(cudaMemsetAsync(comb, 0, sizeof(int32_t) * n, g->stream));  // allocCombineData(cn_combine, 0)
-  VcCountIn vc{cn, scat, comb};
+  double* stat;
+  GRE_CHECK(ws_array(g, WS_COUNTERS, 8, &stat));
+  VcCountIn vc{cn, scat, comb, stat, st ? &st->plugin_count : nullptr};
   SourceSet all;
   all.all = true;
   GRE_CHECK(run_engine(g, vc, dir, all, max_supersteps, scratch, st, nullptr, nullptr));
@@ -264,7 +268,9 @@ int gre_vc_cc(gre_graph g, uint32_t* label, gre_stats* st) {
   RunTimer timer(g);
   GRE_CUDA(cudaMemsetAsync(cc, 0xff, sizeof(uint32_t) * n, g->stream));
   GRE_CUDA(cudaMemsetAsync(comb, 0xff, sizeof(uint32_t) * n, g->stream));
-  VcCC vc{cc, scat, comb, g->perm};
+  double* stat;
+  GRE_CHECK(ws_array(g, WS_COUNTERS, 8, &stat));
+  VcCC vc{cc, scat, comb, g->perm, stat, st ? &st->plugin_count : nullptr};
   SourceSet all;
   all.all = true;
   GRE_CHECK(run_engine(g, vc, GRE_DIR_INOUT, all, 1024, scratch, st, nullptr, nullptr));

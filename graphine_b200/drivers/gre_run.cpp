@@ -136,7 +136,8 @@ static int run_partitioned(const std::string& algo, const std::string& prefix, i
 
 int main(int argc, char** argv) {
   if (argc < 3) {
-    fprintf(stderr, "usage: %s pagerank|pagerank_iter|pagerank_delta|bfs|sssp|sssp1|cc|cin|bc prefix [ascii] [edgelists]\n"
+    fprintf(stderr, "usage: %s pagerank|pagerank_iter|pagerank_delta|bfs|sssp|sssp1|cc|cin|bc prefix [ascii] "
+                    "[edgelists|partition [nparts]]\n"
                     "       %s part_bfs|part_sssp|part_cc|part_pagerank|part_pagerank_iter prefix --ranks P --rank r --id-file F [--device d]\n",
             argv[0], argv[0]);
     return 2;
@@ -153,8 +154,13 @@ int main(int argc, char** argv) {
   try {
     gre::DistributedGraph g;
     const bool in_out = algo == "bfs" || algo == "cc" || algo == "bc" || algo == "cin";
-    if (in_out) g.ingress<gre::InOut>(prefix);
-    else g.ingress<gre::Out>(prefix);
+    // format and method as the reference drivers take them (usr/test_bfs.cpp:40-47); a saved
+    // partition set also needs its part count (the reference's rank count)
+    const std::string format = argc > 3 ? argv[3] : "ascii";
+    const std::string method = argc > 4 ? argv[4] : "edgelists";
+    const uint32_t nparts = argc > 5 ? (uint32_t)strtoul(argv[5], nullptr, 10) : 1u;
+    if (in_out) g.ingress<gre::InOut>(prefix, format, method, false, false, 0, nparts);
+    else g.ingress<gre::Out>(prefix, format, method, false, false, 0, nparts);
     std::vector<uint32_t> roots(1024);
     uint32_t nroots = 0;
     if (algo == "bfs" || algo == "sssp" || algo == "sssp1" || algo == "bc") {
@@ -175,10 +181,8 @@ int main(int argc, char** argv) {
       engine.configMaxSupersteps(algo == "pagerank" ? 10 : 20);  // usr/test_pagerank.cpp:70
       engine.run<gre::Out>(src);
       st = engine.stats();
-      double sum = 0;
-      for (double x : pr.pr) sum += x;
       print_supersteps(st);
-      printf("Sum of pr: %.15g\n", sum);
+      printf("Sum of pr: %.15g\n", st.plugin_value);  // the plugin's output_statistics
     } else if (algo == "pagerank_delta") {  // usr/test_pagerank.cpp:22 with the PageRank_delta typedef
       src.setALL();
       gre::PageRank_delta pr(g);
@@ -207,9 +211,7 @@ int main(int argc, char** argv) {
       engine.run<gre::In>(src);
       st = engine.stats();
       print_supersteps(st);
-      long total = 0;
-      for (int32_t c : cin.cn) total += c;
-      printf("Number of in edges: %ld\n", total);
+      printf("Number of in edges: %llu\n", (unsigned long long)st.plugin_count);  // output_statistics
     } else if (algo == "bfs") {
       src.addVertex(roots[0], g);
       gre::BFS bfs(g);
@@ -234,9 +236,7 @@ int main(int argc, char** argv) {
       engine.run<gre::InOut>(src);
       st = engine.stats();
       print_supersteps(st);
-      long comps = 0;
-      for (size_t v = 0; v < cc.cc.size(); ++v) comps += cc.cc[v] == v;
-      printf("Number of components: %ld\n", comps);
+      printf("Number of components: %llu\n", (unsigned long long)st.plugin_count);  // output_statistics
     } else if (algo == "bc") {
       for (uint32_t r : roots) src.addVertex(r, g);
       gre::BC bc(g);

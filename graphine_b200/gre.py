@@ -65,6 +65,8 @@ class _Stats(C.Structure):
         ("algo_bytes", C.c_uint64),
         ("device_ms", C.c_double),
         ("active", C.c_uint64 * MAX_RECORDED),
+        ("plugin_value", C.c_double),
+        ("plugin_count", C.c_uint64),
     ]
 
 
@@ -78,11 +80,13 @@ class Stats:
     traversed_edges: int = 0
     algo_bytes: int = 0
     device_ms: float = 0.0
+    plugin_value: float = 0.0  # output_statistics: PageRank's sum of ranks
+    plugin_count: int = 0      # output_statistics: CC's number of components
 
     @classmethod
     def _from(cls, s: _Stats) -> "Stats":
         return cls(s.supersteps, list(s.active[: s.n_recorded]), s.arcs_traversed, s.traversed_edges,
-                   s.algo_bytes, s.device_ms)
+                   s.algo_bytes, s.device_ms, s.plugin_value, s.plugin_count)
 
     @property
     def gteps(self) -> float:

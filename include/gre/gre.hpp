@@ -43,16 +43,26 @@ class DistributedGraph {
   ~DistributedGraph() {
     if (g_) gre_graph_free(g_);
   }
-  // ingress<dir>(comm, pool, prefix, "ascii", "edgelists"); `symmetric` lets the CSR serve as
-  // CSC, `reorder` stores vertices by decreasing degree (invisible to callers).
+  // ingress<dir>(comm, pool, prefix, format, method) (DistributedGraph.hpp:153-172):
+  //   method "edgelists": the text files <prefix>.meta + <prefix>.edges.<i>;
+  //   method "partition" / "partitions": the saved partitions <prefix>.part.<nparts>.<r> of an
+  //   np = nparts run (GraphIngress.hpp:86-96, 1024-1071; the reference sets nparts to its rank
+  //   count), merged into this one graph.  Like the reference, partitions hold out-arcs, so
+  //   dir In is refused (GraphIngress.hpp:92-95).
+  // `symmetric` lets the CSR serve as CSC, `reorder` stores vertices by decreasing degree
+  // (invisible to callers).
   template <Dir dir>
   bool ingress(const std::string& prefix, const std::string& format = "ascii", const std::string& method = "edgelists",
-               bool symmetric = false, bool reorder = false, int device = 0) {
-    if (format != "ascii" || method != "edgelists") throw Error(GRE_NOT_IMPLEMENTED, "ingress: only ascii edgelists");
+               bool symmetric = false, bool reorder = false, int device = 0, uint32_t nparts = 1) {
+    const bool parts = method == "partition" || method == "partitions";
+    if (format != "ascii" || !(parts || method == "edgelists"))
+      throw Error(GRE_NOT_IMPLEMENTED, "ingress: ascii edge lists or saved partitions only");
+    if (parts && dir == In) throw Error(GRE_NOT_IMPLEMENTED, "ingress: partitions of In edges are not supported");
     if (g_) gre_graph_free(g_);
     g_ = nullptr;
     uint32_t flags = (uint32_t)dir | (symmetric ? GRE_GRAPH_SYMMETRIC : 0u) | (reorder ? GRE_GRAPH_REORDER : 0u);
-    check(gre_graph_load(prefix.c_str(), flags, device, &g_), "gre_graph_load");
+    if (parts) check(gre_graph_load_parts(prefix.c_str(), nparts, flags, device, &g_), "gre_graph_load_parts");
+    else check(gre_graph_load(prefix.c_str(), flags, device, &g_), "gre_graph_load");
     return true;
   }
   size_t get_num_masters() const { return info().first; }

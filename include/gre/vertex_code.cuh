@@ -12,6 +12,8 @@
 //   __device__ bool apply(uint32_t lv);                         // true: lv becomes active
 //   __device__ bool assert_to_halt(uint32_t lv);                // true: lv leaves the frontier
 //   void reduce();                                              // host, once per superstep
+//   void output_statistics(const EngineContext&);               // host, once after the run
+//                                                               // (optional)
 //
 // The reference's combine receives a striped spin lock (Util/vLock.hpp:75-99); on the device
 // combine is written with atomics (atomicAdd / atomicMin / atomicCAS) and takes no lock.
@@ -30,6 +32,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 namespace gre {
@@ -61,7 +65,23 @@ struct SendCtx {
   }
 };
 
+// What the engine hands output_statistics (the reference passes its DistributedContext,
+// VertexCode.hpp:68-70): the stream the run used and the run's counters.
+struct EngineContext {
+  cudaStream_t stream;
+  uint64_t n;
+  long supersteps;
+  uint64_t arcs_scanned;
+};
+
 namespace vc_detail {
+
+// output_statistics is optional, as in the reference (VertexCode.hpp:68-70 is an empty default)
+template <class VC, class = void>
+struct has_output_statistics : std::false_type {};
+template <class VC>
+struct has_output_statistics<VC, std::void_t<decltype(std::declval<VC&>().output_statistics(
+                                     std::declval<const EngineContext&>()))>> : std::true_type {};
 
 template <class VC>
 __global__ void k_init_all(VC vc, uint64_t n, uint32_t* curr_bits) {
@@ -241,6 +261,8 @@ class SynchronousEngine {
       if (count == 0) break;
     }
     superstep_ = ss;
+    // run_master calls output_statistics once the loop has ended (Engine.hpp:402-404)
+    if constexpr (vc_detail::has_output_statistics<VC>::value) vc_.output_statistics(EngineContext{stream_, n, ss, arcs_});
     return cudaGetLastError();
   }
 

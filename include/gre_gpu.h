@@ -76,6 +76,12 @@ typedef struct gre_stats {
   uint64_t algo_bytes;     /* algorithmic HBM bytes of the run (byte model of each kernel) */
   double device_ms;        /* device time of the run, CUDA events on the graph's stream */
   uint64_t active[GRE_MAX_RECORDED_SUPERSTEPS];
+  /* The plugin's output_statistics (VertexCode.hpp:70), which the engine calls once after the
+   * last superstep (Engine.hpp:404), for the gre_vc_* runs: PageRank plugins report the sum of
+   * the ranks (Kernels/PageRank.hpp:102-124), ConnectedComponents the number of components
+   * (Kernels/CC.hpp:98-120); 0 for the other plugins and the fast paths. */
+  double plugin_value;
+  uint64_t plugin_count;
 } gre_stats;
 
 typedef struct gre_graph_s* gre_graph;
@@ -204,11 +210,12 @@ int gre_bfs(gre_graph g, const uint32_t* srcs, uint32_t nsrc, int32_t* levels, g
 /* No counterpart in the reference.  gre_bfs for callers that cannot let the library allocate
  * device memory (a process whose device memory is reserved and capped by its own pool
  * allocator, or a latency-critical loop that cannot take cudaMalloc's implicit device
- * synchronisation): one source, `level` must be device memory (n int32), and all scratch lives
- * in a fixed 32 MiB array inside the library, so graphs are limited to 1,048,576 vertices
- * (larger ones: GRE_INVALID_ARG).  The array is shared by all calls on a device: calls that
- * overlap on the GPU race.  The first call on a device looks up the array's address; make it
- * before any stream capture. */
+ * synchronisation): one source, `level` must be device memory of the graph's device (n int32;
+ * anything else: GRE_INVALID_ARG), and all scratch lives in a fixed 32 MiB array inside the
+ * library, so graphs are limited to 1,048,576 vertices (larger ones: GRE_INVALID_ARG).  The
+ * array is shared by all calls on a device: calls that overlap on the GPU race.  The first call
+ * on a device looks up the array's address, and so does the first call after that device's
+ * context was replaced (cudaDeviceReset); make those calls before any stream capture. */
 int gre_bfs_noalloc(gre_graph g, uint32_t src, int32_t* level, gre_stats* st);
 /* Multi-source BFS with 64 sources per uint64 frontier word.  levels: nsrc x n int32. */
 int gre_msbfs(gre_graph g, const uint32_t* srcs, uint32_t nsrc, int32_t* levels, gre_stats* st);

@@ -59,6 +59,11 @@ def lib() -> C.CDLL:
             "oracle_pagerank_delta": (I32, [P, U32, P, P, U32, C.POINTER(U32)]),
             "oracle_sssp1": (I32, [P, U32, U64, P, P, P, P, U32, C.POINTER(U32)]),
             "oracle_count_in": (I32, [P, I32, U32, P, P, U32, C.POINTER(U32)]),
+            "oracle_rmat": (I32, [U32, U32, U64, I32, C.POINTER(U64), C.POINTER(U64), C.POINTER(P), C.POINTER(P)]),
+            "oracle_host_free": (None, [P]),
+            "oracle_write_edgelists": (I32, [C.c_char_p, U64, U64, P, P, U32]),
+            "oracle_write_roots": (I32, [C.c_char_p, P, U32]),
+            "oracle_sssp_weights_csr": (None, [U64, U64, P, P, P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -227,6 +232,66 @@ class Restatement:
 
 def sssp_weight(wseed: int, u: int, v: int) -> int:
     return int(lib().oracle_sssp_weight(wseed, u, v))
+
+
+def sssp_weights_csr(wseed: int, off: np.ndarray, col: np.ndarray) -> np.ndarray:
+    """The harness SSSP weight of every arc of a CSR, in CSR order (uint32)."""
+    off = np.ascontiguousarray(off, dtype=np.uint64)
+    col = np.ascontiguousarray(col, dtype=np.uint32)
+    w = np.empty(max(len(col), 1), dtype=np.uint32)
+    lib().oracle_sssp_weights_csr(wseed, len(off) - 1, _p(off), _p(col), _p(w))
+    return w[: len(col)]
+
+
+# ----------------------------------------------------------------------------------------------
+# inputs, generated on the host without the product library (oracle/inputs.cpp)
+# ----------------------------------------------------------------------------------------------
+def rmat(scale: int, edgefactor: int = 16, seed: int = 1, symmetric: bool = True):
+    """Seeded RMAT CSR: (n, off uint64[n+1], col uint32[m]); the same graph as the product's
+    generator for the same arguments."""
+    n, m = C.c_uint64(), C.c_uint64()
+    po, pc = C.c_void_p(), C.c_void_p()
+    st = lib().oracle_rmat(scale, edgefactor, seed, int(symmetric), C.byref(n), C.byref(m), C.byref(po), C.byref(pc))
+    if st:
+        raise RuntimeError(f"oracle_rmat({scale}, {edgefactor}, {seed}) failed: {st}")
+    try:
+        off = np.ctypeslib.as_array(C.cast(po, C.POINTER(C.c_uint64)), shape=(n.value + 1,)).copy()
+        col = np.ctypeslib.as_array(C.cast(pc, C.POINTER(C.c_uint32)), shape=(max(m.value, 1),))[: m.value].copy()
+    finally:
+        lib().oracle_host_free(po)
+        lib().oracle_host_free(pc)
+    return n.value, off, col
+
+
+def write_edgelists(prefix: str, n: int, off: np.ndarray, col: np.ndarray, nfiles: int = 4) -> None:
+    off = np.ascontiguousarray(off, dtype=np.uint64)
+    col = np.ascontiguousarray(col, dtype=np.uint32)
+    st = lib().oracle_write_edgelists(prefix.encode(), n, len(col), _p(off), _p(col) if len(col) else None, nfiles)
+    if st:
+        raise RuntimeError(f"oracle_write_edgelists({prefix}) failed: {st}")
+
+
+def write_roots(prefix: str, roots) -> None:
+    r = np.ascontiguousarray(roots, dtype=np.uint32)
+    st = lib().oracle_write_roots(prefix.encode(), _p(r), len(r))
+    if st:
+        raise RuntimeError(f"oracle_write_roots({prefix}) failed: {st}")
+
+
+def sample_sources(off: np.ndarray, k: int, seed: int) -> np.ndarray:
+    """k distinct vertices with at least one arc, drawn with a seeded generator (sorted)."""
+    deg = np.diff(off.astype(np.int64))
+    cand = np.flatnonzero(deg > 0)
+    if len(cand) <= k:
+        return cand.astype(np.uint32)
+    return np.sort(np.random.default_rng(seed).choice(cand, size=k, replace=False)).astype(np.uint32)
+
+
+def reached_edges(off: np.ndarray, level: np.ndarray) -> int:
+    """Graph500 numerator of a BFS/SSSP run on a symmetric graph: undirected edges with both
+    endpoints reached (= half the arcs out of reached vertices)."""
+    deg = np.diff(off.astype(np.int64))
+    return int(deg[np.asarray(level) >= 0].sum() // 2)
 
 
 # ----------------------------------------------------------------------------------------------

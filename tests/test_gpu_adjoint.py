@@ -38,7 +38,9 @@ def dense_P(n, off, col, w):
 
 @pytest.mark.parametrize("reorder", [False, True], ids=["plain", "relabelled"])
 def test_weighted_forward_and_adjoint_vs_dense_solve(reorder):
-    n, off, col, w, g = weighted_graph(10, 3, directed=True, reorder=reorder)
+    """The differentiation config's dense check: a directed RMAT-12 graph (4096 vertices) with
+    lognormal weights, forward and adjoint against LU solves of the dense FP64 systems."""
+    n, off, col, w, g = weighted_graph(12, 3, directed=True, reorder=reorder)
     rng = np.random.default_rng(1)
     pers = rng.random(n) + 0.5
     c = rng.standard_normal(n)
@@ -165,3 +167,54 @@ def test_autograd_function_matches_dense_gradient():
     gw_ref = D * r_ref[src] / s[src] * (lam[col] - (P @ lam)[src])
     assert rel_l1(gw.numpy(), gw_ref) <= 1e-6
     assert rel_l1(gp.numpy(), (1 - D) * lam) <= 1e-6
+
+
+def test_adjoint_vs_central_differences_s20_1000_edges():
+    """The differentiation config as stated: RMAT-20 (EF16, symmetric, relabelled) with lognormal
+    (0, 1) arc weights, L = c . r with c ~ N(0, 1); dL/dW on 1000 random arcs against FP64 central
+    differences with h = 1e-6.
+
+    Both solves of a difference run the same fixed number of Jacobi steps (tol = 0, 230 steps:
+    0.85^230 < 1e-16, converged to rounding), so they take the same summation path, and
+    L(w+h) - L(w-h) is formed as c . (r+ - r-) so that no large sum cancels.  What is left is
+    rounding noise in r (a few ulps per vertex, uncorrelated between vertices) carried into the
+    difference quotient: noise ~ eps * ||c * r||_2 / h.  The per-arc tolerance is 64x that floor
+    plus 1e-5 relative (the O(h^2) truncation term is below 1e-10 relative here)."""
+    import torch
+
+    n, off, col = G.rmat_host(20, 16, 41, True)
+    rng = np.random.default_rng(41)
+    w = np.exp(rng.standard_normal(len(col)))
+    g = G.Graph.from_csr(n, off, col, dir=G.InOut, symmetric=True, reorder=True)
+    dev = torch.device("cuda", 0)
+    wd = torch.tensor(w, dtype=torch.float64, device=dev)
+    g.set_weights_f64(wd)
+    c = rng.standard_normal(n)
+    steps = 230
+    r = torch.empty(n, dtype=torch.float64, device=dev)
+    G.pagerank_weighted(g, D, None, tol=0.0, max_iters=steps, out=r)
+    r_h = r.cpu().numpy()
+    _, _, gw, _, _ = G.pagerank_adjoint(g, r_h, c, D, tol=0.0, max_iters=steps)
+    h = 1e-6
+    arcs = rng.choice(len(col), size=1000, replace=False)
+    ct = torch.tensor(c, dtype=torch.float64, device=dev)
+    rp, rm = torch.empty_like(r), torch.empty_like(r)
+    fd = np.empty(len(arcs))
+    for i, a in enumerate(arcs):
+        a = int(a)
+        base = float(w[a])
+        wd[a] = base + h
+        g.set_weights_f64(wd)
+        G.pagerank_weighted(g, D, None, tol=0.0, max_iters=steps, out=rp)
+        wd[a] = base - h
+        g.set_weights_f64(wd)
+        G.pagerank_weighted(g, D, None, tol=0.0, max_iters=steps, out=rm)
+        wd[a] = base
+        fd[i] = float(torch.dot(ct, rp - rm)) / (2 * h)
+    g.set_weights_f64(wd)
+    eps = np.finfo(np.float64).eps
+    floor = eps * float(np.linalg.norm(c * r_h)) / h
+    tol = 64 * floor + 1e-5 * np.abs(gw[arcs])
+    err = np.abs(fd - gw[arcs])
+    assert np.all(err <= tol), (float(err.max()), float(floor), int(np.argmax(err / tol)))
+    assert rel_l1(fd, gw[arcs]) <= 1e-4, rel_l1(fd, gw[arcs])

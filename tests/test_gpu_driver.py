@@ -10,6 +10,7 @@ import numpy as np
 import pytest
 
 import graphine_b200.gre as G
+import oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -90,3 +91,26 @@ def test_partitioned_driver_one_rank(golden):
         assert p.returncode == 0, p.stderr
         lab, _ = G.cc(g)
         assert f"Number of components: {int((lab == np.arange(n)).sum())}" in p.stdout
+
+
+def test_driver_ingress_from_saved_partitions():
+    """`gre_run <algo> <prefix> ascii partition P` reads the saved partitions <prefix>.part.P.<r>
+    (the reference's ingress method "partition", GraphIngress.hpp:86-96, 1024-1071) instead of the
+    edge-list text, and runs as on the same graph loaded from text."""
+    n, off, col = G.rmat_host(11, 8, 4, True)
+    src = np.repeat(np.arange(n, dtype=np.int64), np.diff(off.astype(np.int64)))
+    cut = np.random.default_rng(2).integers(0, 3, len(col))
+    with tempfile.TemporaryDirectory() as td:
+        prefix = os.path.join(td, "p")
+        open(prefix + ".meta", "w").write(f"{n} {len(col)}\n")
+        for r in range(3):
+            pairs = np.stack([src[cut == r], col[cut == r].astype(np.int64)], axis=1).astype(np.uint64)
+            pairs.tofile(prefix + f".part.3.{r}")
+        p = subprocess.run([DRIVER, "cc", prefix, "ascii", "partition", "3"], capture_output=True, text=True, timeout=300)
+        assert p.returncode == 0, p.stderr
+        p2 = subprocess.run([DRIVER, "bfs", prefix, "ascii", "partitions", "3"], capture_output=True, text=True,
+                            timeout=300)
+        assert p2.returncode != 0  # no .roots file: the reference driver's message and a status
+        assert "Err in reading src vertex" in p2.stderr
+    lab, _ = O.Restatement.from_csr(n, off, col).cc()
+    assert f"Number of components: {int((lab == np.arange(n)).sum())}" in p.stdout

@@ -127,3 +127,20 @@ def test_graph_batch_run_equals_per_graph_calls():
     with pytest.raises(G.GreError) as e:
         G.graph_batch_run(gs, 7)
     assert e.value.status == G.GRE_INVALID_ARG
+
+
+@pytest.mark.parametrize("batched", [False, True], ids=["looped", "batched"])
+def test_bc_on_a_long_path(batched):
+    """A path of 6000 vertices: BFS levels run past 4096 from an end, and BC (looped and batched)
+    still equals the oracle's (every interior vertex's dependency counts the vertices beyond it)."""
+    n = 6000
+    edges = [(i, i + 1) for i in range(n - 1)] + [(i + 1, i) for i in range(n - 1)]
+    off, col = csr(n, edges)
+    g = G.Graph.from_csr(n, off, col, dir=G.InOut, symmetric=True)
+    R = O.Restatement.from_csr(n, off, col)
+    roots = np.array([0, 2500, n - 1], np.uint32)
+    ref, _ = R.bc(roots)
+    got, st = G.bc(g, roots, batched=batched)
+    assert rel_l1(got, ref) <= TOL
+    lv, _ = G.bfs(g, roots[:1])
+    assert lv.max() == n - 1

@@ -6,8 +6,9 @@ the checker here; the oracle is too slow at this size):
   most; every other reached vertex has a neighbour one level up.
 * SSSP (random uint32 weights in [1, 255]): no arc can shorten a distance; every reached
   non-root vertex has a tight arc (dist[u] + w == dist[v]).
-* CC: labels constant along arcs, a label is a member of its component (its own label) and no
-  larger than any member's id, i.e. the smallest caller id.
+* CC: labels constant along arcs, no larger than the vertex's id, the label's vertex labelled
+  with itself, and a BFS from all self-labelled vertices reaching every vertex (so every label
+  lies in its own component and is its smallest caller id).
 * PageRank: superstep 21 recomputed from superstep 20 with an independent scatter-add in FP64
   (relative L1 difference <= 1e-12).
 * The 1D-partitioned paths (two parts as threads on this GPU) equal the one-GPU results.
@@ -115,6 +116,12 @@ def test_full_size_cc_properties(big):
     ids = torch.arange(g.n, device=off.device)
     assert bool((Lb <= ids).all())
     assert bool((Lb[Lb] == Lb).all())
+    # a BFS from every self-labelled vertex reaches all vertices: with labels constant along arcs,
+    # each vertex's label then lies in its own component (two components cannot share a label)
+    roots = torch.nonzero(Lb == ids).flatten().to(torch.int32)
+    lv = torch.empty(g.n, dtype=torch.int32, device=off.device)
+    G.bfs_multiroot(g, roots, out=lv)
+    assert bool((lv >= 0).all())
 
 
 def test_full_size_pagerank_superstep(big):
@@ -140,16 +147,20 @@ def test_full_size_partitioned_equals_one_gpu(big):
 
     g, off, col, deg = big
     root = int(torch.nonzero(deg > 0)[1000].item())
+    g.set_weights_hash(7)
     one_lv, _ = G.bfs(g, [root])
     one_pr, _ = G.pagerank(g, G.PR_ITER, 0.85, 20)
     one_cc, _ = G.cc(g)
+    one_d, _ = G.sssp(g, [root])
+    # two parts: each part's rows still reach the CTA and hub-chunk bins of the degree schedule
     out = PT.run_local(g, 2, lambda part, x: (part.bfs(root, x)[0], part.pagerank(x, G.PR_ITER, 0.85, 20)[0],
-                                              part.cc(x)[0]))
+                                              part.cc(x)[0], part.sssp(root, x)[0]))
     windows = g.row_schedule()[3] != 0  # source windows: a different association order per row
-    for lv, pr, lab in out:
+    for lv, pr, lab, dist in out:
         np.testing.assert_array_equal(lv, one_lv)
         if windows:
             assert np.abs(pr - one_pr).sum() <= 1e-12 * np.abs(one_pr).sum()
         else:
             np.testing.assert_array_equal(pr, one_pr)
         np.testing.assert_array_equal(lab, one_cc)
+        np.testing.assert_array_equal(dist, one_d)

@@ -468,28 +468,47 @@ def test_s20_bfs_properties(rmat20):
 
 
 def test_s20_sssp_properties(rmat20):
+    """A complete certificate of the distances at scale 20: no arc can shorten a distance (every
+    arc checked), every reached vertex other than the root has a tight arc, and the reached set
+    is the BFS's.  The weights are recomputed on the host by the oracle's restatement."""
     g, off, col, src = rmat20
     g.set_weights_hash(31)
     r = int(G.sample_sources(off, 1, 8)[0])
     d, _ = G.sssp(g, [r])
-    lo = np.minimum(src, col).astype(np.uint64)
-    hi = np.maximum(src, col).astype(np.uint64)
-    # weights recomputed on the host through the oracle's independent restatement
-    wt = np.array([O.sssp_weight(31, int(u), int(v)) for u, v in zip(lo[:2000], hi[:2000])], dtype=np.int64)
+    wt = O.sssp_weights_csr(31, off, col).astype(np.int64)
     du, dv = d[src].astype(np.int64), d[col].astype(np.int64)
     inf = 0xFFFFFFFF
-    sel = (du[:2000] != inf)
-    assert np.all(dv[:2000][sel] <= du[:2000][sel] + wt[sel])
+    assert d[r] == 0
+    fin = du != inf
+    assert np.all(dv[fin] <= du[fin] + wt[fin])
+    tight = np.zeros(g.n, dtype=bool)
+    tight[col[fin & (dv == du + wt)]] = True
+    reached = d != inf
+    reached[r] = False
+    assert np.all(tight[reached])
     dl, _ = G.bfs(g, [r])
     assert np.all((d == inf) == (dl < 0))
+
+
+def cc_certificate(g, lab, src, col):
+    """Labels are the minimum-id labelling of the components: (1) constant along every arc,
+    (2) no larger than the vertex's own id, (3) the label's vertex is labelled with itself, and (4)
+    a BFS from all self-labelled vertices reaches every vertex.  By (1) a vertex reached from r
+    carries r's label r, so (4) puts every vertex's label inside its own component, and (2) then
+    makes it the component's smallest id.  (Without (4), two components could share one label.)"""
+    ids = np.arange(g.n)
+    assert np.all(lab[src] == lab[col])
+    assert np.all(lab <= ids)
+    assert np.all(lab[lab] == lab)
+    roots = np.flatnonzero(lab == ids).astype(np.uint32)
+    lv, _ = G.bfs_multiroot(g, roots)
+    assert np.all(lv >= 0)
 
 
 def test_s20_cc_properties(rmat20):
     g, off, col, src = rmat20
     lab, _ = G.cc(g)
-    assert np.all(lab[src] == lab[col])
-    assert np.all(lab <= np.arange(g.n))
-    assert np.all(lab[lab] == lab)
+    cc_certificate(g, lab, src, col)
     lab2, _ = G.vc_cc(g)
     np.testing.assert_array_equal(lab, lab2)
 
@@ -506,3 +525,21 @@ def test_sssp_relaxation_forms_agree(monkeypatch, binned):
         roots = G.sample_sources(off, 3, 1)
         ref = R.sssp_many(roots, 3)
         np.testing.assert_array_equal(G.sssp(g, roots)[0].reshape(len(roots), n), ref)
+
+
+@pytest.mark.parametrize("name", SYM)
+@REORDER
+def test_plugin_output_statistics(golden, name, reorder):
+    """The engine calls each plugin's output_statistics once after the last superstep
+    (Engine.hpp:404): PageRank reports the sum of its ranks, CountIn the number of in-edges, CC the
+    number of components, as the reference plugins print them."""
+    case = golden[name]
+    g = graph_of(case, reorder)
+    pr, st = G.vc_pagerank(g, G.PR_REFERENCE, 10)
+    assert abs(st.plugin_value - float(np.sum(case["pr_gre10"]))) <= 1e-12 * float(np.sum(case["pr_gre10"]))
+    cn, st = G.vc_count_in(g, G.In, 1)
+    assert st.plugin_count == int(case["countin"].astype(np.int64).sum())
+    lab, st = G.vc_cc(g)
+    assert st.plugin_count == int(np.sum(case["cc_label"] == np.arange(int(case["n"]))))
+    _, st = G.cc(g)  # the fast paths run no plugin
+    assert st.plugin_count == 0 and st.plugin_value == 0.0

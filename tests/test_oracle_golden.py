@@ -141,6 +141,33 @@ def test_weight_function_matches_product():
         assert w == G.sssp_weight(99, u, v)
 
 
+@pytest.mark.parametrize("scale,sym,seed", [(10, True, 7), (12, False, 3), (16, True, 26)])
+def test_oracle_inputs_match_product_generator(scale, sym, seed):
+    """The oracle's own RMAT restatement (oracle/inputs.cpp, used by the CPU reference arm so that
+    it loads no product code) gives the product generator's graph arc for arc; its text files and
+    per-arc weights match the product's too."""
+    n, off, col = O.rmat(scale, 16, seed, sym)
+    n2, off2, col2 = G.rmat_host(scale, 16, seed, sym)
+    assert n == n2
+    np.testing.assert_array_equal(off, off2)
+    np.testing.assert_array_equal(col, col2)
+    w = O.sssp_weights_csr(5, off, col)
+    src = np.repeat(np.arange(n, dtype=np.int64), np.diff(off.astype(np.int64)))
+    pick = np.random.default_rng(1).choice(len(col), size=200, replace=False)
+    assert all(int(w[a]) == G.sssp_weight(5, int(src[a]), int(col[a])) for a in pick)
+    if scale <= 12:
+        with tempfile.TemporaryDirectory() as td:
+            a, b = os.path.join(td, "a"), os.path.join(td, "b")
+            O.write_edgelists(a, n, off, col, 4)
+            G.write_edgelists(b, n, off, col, 4)
+            for suffix in [".meta"] + [f".edges.{i}" for i in range(4)]:
+                assert open(a + suffix).read() == open(b + suffix).read()
+            roots = O.sample_sources(off, 5, 3)
+            np.testing.assert_array_equal(roots, G.sample_sources(off, 5, 3))
+            O.write_roots(a, roots)
+            np.testing.assert_array_equal(G.read_roots(a), roots)
+
+
 # ---------------------------------------------------------------------------------------------
 # the other reference plugins: PageRank_delta, SSSP1 (predecessors), CountIn
 # ---------------------------------------------------------------------------------------------

@@ -7,8 +7,9 @@ synchronisation of cudaMalloc / cudaFree.  Its scratch is a fixed array inside t
 
 Checked through the C ABI: the levels equal those of gre_bfs (bit-exact, as every integer
 result here) on two calls in a row that share the scratch, on a plain and a relabelled graph;
-the calls change no free device memory; graphs beyond the scratch's 1,048,576 vertices and host
-output buffers are rejected.  This file is collected last so that a run stopping at the first
+the calls change no free device memory; graphs beyond the scratch's 1,048,576 vertices and
+output buffers that are not device memory of the graph's device (pageable or pinned host memory)
+are rejected.  This file is collected last so that a run stopping at the first
 failure has already run every other test.
 """
 import ctypes
@@ -59,3 +60,6 @@ def test_noalloc_rejects_oversize_graph_and_host_output():
     small = G.Graph.rmat(10, 8, 1, True)
     host = np.empty(small.n, dtype=np.int32)
     assert G.lib().gre_bfs_noalloc(small._h, 0, host.ctypes.data, None) == G.GRE_INVALID_ARG
+    pinned = torch.empty(small.n, dtype=torch.int32, pin_memory=True)  # host memory the GPU can map
+    assert G.lib().gre_bfs_noalloc(small._h, 0, pinned.data_ptr(), None) == G.GRE_INVALID_ARG
+    assert "graph's device" in G.last_error()
