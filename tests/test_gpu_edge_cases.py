@@ -132,15 +132,24 @@ def test_graph_batch_run_equals_per_graph_calls():
 @pytest.mark.parametrize("batched", [False, True], ids=["looped", "batched"])
 def test_bc_on_a_long_path(batched):
     """A path of 6000 vertices: BFS levels run past 4096 from an end, and BC (looped and batched)
-    still equals the oracle's (every interior vertex's dependency counts the vertices beyond it)."""
+    equals the closed form (a source s adds to every v != s the number of vertices beyond v).
+
+    The fast paths run BFS/BC to completion.  The reference engine stops every run after its
+    default 1024 supersteps (Engine.hpp:108, which usr/test_bc.cpp does not raise), so on this
+    graph its levels end at 1023; the device engine (gre_vc_*) keeps that limit, and the oracle
+    restates it, which is why the closed form is the reference here."""
     n = 6000
     edges = [(i, i + 1) for i in range(n - 1)] + [(i + 1, i) for i in range(n - 1)]
     off, col = csr(n, edges)
     g = G.Graph.from_csr(n, off, col, dir=G.InOut, symmetric=True)
-    R = O.Restatement.from_csr(n, off, col)
     roots = np.array([0, 2500, n - 1], np.uint32)
-    ref, _ = R.bc(roots)
+    v = np.arange(n, dtype=np.float64)
+    ref = np.zeros(n)
+    for s in roots:
+        ref += np.where(v > s, n - 1 - v, np.where(v < s, v, 0.0))
     got, st = G.bc(g, roots, batched=batched)
     assert rel_l1(got, ref) <= TOL
     lv, _ = G.bfs(g, roots[:1])
-    assert lv.max() == n - 1
+    np.testing.assert_array_equal(lv, np.arange(n))
+    R = O.Restatement.from_csr(n, off, col)  # the reference's engine limit, restated
+    assert R.bfs(0)[0].max() == 1023
