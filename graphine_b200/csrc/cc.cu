@@ -23,37 +23,9 @@
 
 #include "gre_internal.cuh"
 #include "rows.cuh"
+#include "uf.cuh"
 
 namespace gre {
-
-__device__ __forceinline__ uint32_t uf_find(uint32_t* parent, uint32_t x) {
-  uint32_t p = parent[x];
-  while (p != x) {
-    const uint32_t gp = parent[p];
-    if (gp != p) parent[x] = gp;  // path halving (benign race: gp is an ancestor)
-    x = p;
-    p = gp;
-  }
-  return x;
-}
-
-// key(x): the caller's vid of internal vertex x (relabelled graphs) - roots are linked by it
-__device__ __forceinline__ uint32_t uf_key(const uint32_t* __restrict__ vid, uint32_t x) { return vid ? __ldg(vid + x) : x; }
-
-__device__ __forceinline__ void uf_union(uint32_t* parent, const uint32_t* __restrict__ vid, uint32_t a, uint32_t b) {
-  while (true) {
-    a = uf_find(parent, a);
-    b = uf_find(parent, b);
-    if (a == b) return;
-    const bool a_hi = uf_key(vid, a) > uf_key(vid, b);
-    const uint32_t hi = a_hi ? a : b;
-    const uint32_t lo = a_hi ? b : a;
-    if (atomicCAS(parent + hi, hi, lo) == hi) return;
-    // hi gained a parent meanwhile: retry from the new roots
-    a = hi;
-    b = lo;
-  }
-}
 
 struct HookArcs {
   const uint32_t* __restrict__ col;
@@ -145,6 +117,19 @@ __global__ void k_count_roots(uint64_t n, const uint32_t* __restrict__ label, un
   if ((threadIdx.x & 31u) == 0 && s) atomicAdd(c, s);
 }
 
+uint32_t uf_most_frequent(std::vector<uint32_t>& hs, uint32_t ns) {
+  std::sort(hs.begin(), hs.begin() + ns);
+  uint32_t best = hs[0], run = 0, best_run = 0;
+  for (uint32_t i = 0; i < ns; ++i) {
+    run = (i && hs[i] == hs[i - 1]) ? run + 1 : 1;
+    if (run > best_run) {
+      best_run = run;
+      best = hs[i];
+    }
+  }
+  return best;
+}
+
 }  // namespace gre
 
 using namespace gre;
@@ -190,15 +175,7 @@ int gre_cc(gre_graph g, uint32_t* label, gre_stats* st) {
     const uint32_t ns = (uint32_t)std::min<uint64_t>(kSample, (n + stride - 1) / stride);
     GRE_CUDA(cudaMemcpyAsync(hs.data(), sample, sizeof(uint32_t) * ns, cudaMemcpyDeviceToHost, g->stream));
     GRE_CUDA(cudaStreamSynchronize(g->stream));
-    std::sort(hs.begin(), hs.begin() + ns);
-    uint32_t best = hs[0], run = 0, best_run = 0;
-    for (uint32_t i = 0; i < ns; ++i) {
-      run = (i && hs[i] == hs[i - 1]) ? run + 1 : 1;
-      if (run > best_run) {
-        best_run = run;
-        best = hs[i];
-      }
-    }
+    const uint32_t best = uf_most_frequent(hs, ns);
     GRE_CUDA(cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), g->stream));
     k_uf_skipbits<<<grid_for((n + 31) >> 5, 256), 256, 0, g->stream>>>(n, parent, g->off, best, kSampled, skip, counts);
     HookArcs rest{g->col, parent, g->perm, false, skip, g->off, kSampled};

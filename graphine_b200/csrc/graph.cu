@@ -766,7 +766,7 @@ int gre_graph_union(const gre_graph* graphs, uint32_t k, int device, gre_graph* 
   if (!graphs || !out || !vertex_offset || k == 0) return GRE_NULL;
   clear_error();
   uint64_t n = 0, m = 0;
-  bool sym = true, all_w32 = true;
+  bool sym = true, all_w32 = true, w32_sym = true;
   for (uint32_t i = 0; i < k; ++i) {
     if (!graphs[i]) return GRE_NULL;
     if (graphs[i]->perm) {
@@ -778,6 +778,7 @@ int gre_graph_union(const gre_graph* graphs, uint32_t k, int device, gre_graph* 
     m += graphs[i]->m;
     sym = sym && graphs[i]->symmetric();
     all_w32 = all_w32 && graphs[i]->w32;
+    w32_sym = w32_sym && graphs[i]->w32_symmetric;
   }
   vertex_offset[k] = n;
   if (n > 0xffffffffull) return GRE_INVALID_ARG;
@@ -789,6 +790,7 @@ int gre_graph_union(const gre_graph* graphs, uint32_t k, int device, gre_graph* 
   GRE_CUDA(cudaMalloc(&g->off, sizeof(uint64_t) * (n + 1)));
   GRE_CUDA(cudaMalloc(&g->col, sizeof(uint32_t) * (m ? m : 1)));
   if (all_w32) GRE_CUDA(cudaMalloc(&g->w32, sizeof(uint32_t) * (m ? m : 1)));
+  g->w32_symmetric = all_w32 && w32_sym && sym;
   uint64_t vb = 0, ab = 0;
   for (uint32_t i = 0; i < k; ++i) {
     gre_graph s = graphs[i];
@@ -868,6 +870,7 @@ int gre_graph_set_weights_u32(gre_graph g, const uint32_t* w) {
   if (!g->w32) GRE_CUDA(cudaMalloc(&g->w32, sizeof(uint32_t) * (g->m ? g->m : 1)));
   GRE_CHECK(upload_arcs(g, w, 4, g->w32));
   g->w32_mean = -1.0;
+  g->w32_symmetric = false;  // explicit per-arc weights: not known to be symmetric
   g->sssp_split.release();
   GRE_CUDA(cudaStreamSynchronize(g->stream));
   return GRE_SUCCESS;
@@ -880,6 +883,7 @@ int gre_graph_set_weights_hash(gre_graph g, uint64_t wseed) {
   if (g->m) k_hash_weights<<<grid_for(g->m, 256), 256, 0, g->stream>>>(g->n, g->m, g->off, g->col, g->perm, wseed, g->w32);
   GRE_LAUNCH_CHECK();
   g->w32_mean = -1.0;
+  g->w32_symmetric = g->symmetric();  // a function of the undirected edge
   g->sssp_split.release();
   GRE_CUDA(cudaStreamSynchronize(g->stream));
   return GRE_SUCCESS;

@@ -134,6 +134,10 @@ struct gre_graph_s {
   // weights
   uint32_t* w32 = nullptr;
   double w32_mean = -1.0;  // mean of w32, computed on first use (-1: unknown)
+  // the weight of every arc u->v equals that of v->u (a symmetric graph with weights of the
+  // undirected edge, as gre_graph_set_weights_hash makes them); lets SSSP pull over a vertex's
+  // own arcs instead of pushing along its neighbours'
+  bool w32_symmetric = false;
   // SSSP light/heavy arc split for bucket width `delta` (sssp.cu): each row's arcs reordered so
   // the light ones (w < delta) come first; heavy ones start at lsplit[v].  Built on first use,
   // dropped when the weights or the arc order change.

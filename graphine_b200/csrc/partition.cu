@@ -41,6 +41,7 @@
 
 #include "gre_internal.cuh"
 #include "rows.cuh"
+#include "uf.cuh"
 
 struct gre_part_s {
   gre_graph sub = nullptr;   // the owned rows; columns are exchange indices
@@ -52,6 +53,7 @@ struct gre_part_s {
   uint32_t delta = 0;        // SSSP bucket width: half the mean weight (0: no buckets)
   uint32_t* xof = nullptr;   // caller id -> exchange index (n)
   uint32_t* xmap = nullptr;  // exchange index -> caller id, 0xffffffff for padding (P * L)
+  uint64_t cc_remote = ~0ull;  // arcs of the owned rows that lead to another rank (counted on first use)
 };
 
 namespace gre {
@@ -247,6 +249,14 @@ struct PartGather {
   const uint32_t* __restrict__ col;
   const double* __restrict__ contrib;  // all P * L slots
   __device__ __forceinline__ double operator()(uint32_t, uint64_t a) const { return __ldg(contrib + __ldg(col + a)); }
+  static constexpr bool kQuad = true;
+  __device__ __forceinline__ void quad(uint32_t, uint64_t a, double x[4]) const {
+    const uint4 c = __ldg((const uint4*)(col + a));
+    x[0] = __ldg(contrib + c.x);
+    x[1] = __ldg(contrib + c.y);
+    x[2] = __ldg(contrib + c.z);
+    x[3] = __ldg(contrib + c.w);
+  }
 };
 
 // pr = tele + d * sum; the power iteration refreshes the owner's contribution pr / outdeg
@@ -364,76 +374,142 @@ __global__ void k_part_sssp_select(uint64_t W, uint32_t* __restrict__ pend, cons
   }
 }
 
-// CC labels start as the caller ids of the slots (padding: none)
-__global__ void k_part_cc_init(uint64_t L, const uint32_t* __restrict__ xmap_rank, uint32_t* __restrict__ lab) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < L; i += (uint64_t)gridDim.x * blockDim.x)
-    lab[i] = xmap_rank[i];
-}
-
-// New label of row v from the smallest neighbour label m (UINT32_MAX: none): the shortcut
-// through the vertices the labels name, and a lower value replaces the label.
-__device__ __forceinline__ bool cc_update(uint32_t v, uint32_t m, const uint32_t* __restrict__ lab_all,
-                                          const uint32_t* __restrict__ xof, uint32_t* __restrict__ lab) {
-  const uint32_t cur = lab[v];
-  if (m != 0xffffffffu) m = min(m, lab_all[xof[m]]);
-  if (cur != 0xffffffffu) m = min(m, lab_all[xof[cur]]);
-  if (m < cur) {
-    lab[v] = m;
-    return true;
+// CC, phase 1: union-find over the arcs whose both ends this rank owns (slots lo .. lo + L - 1
+// in exchange indices), roots linked by the caller id of the slot (key).
+struct HookLocal {
+  const uint32_t* __restrict__ col;  // exchange indices
+  uint32_t* parent;                  // L slots
+  const uint32_t* __restrict__ key;  // caller id of each slot
+  uint32_t lo, L;
+  // Afforest's second pass (symmetric graphs): rows flagged in `skip` are left out and the first
+  // `sampled` arcs of the others were already seen (null: every arc)
+  const uint32_t* __restrict__ skip = nullptr;
+  const uint64_t* __restrict__ off = nullptr;
+  uint32_t sampled = 0;
+  __device__ __forceinline__ double operator()(uint32_t u, uint64_t a) const {
+    if (skip) {
+      if ((__ldg(skip + (u >> 5)) >> (u & 31u)) & 1u) return 0.0;
+      if (a < __ldg(off + u) + sampled) return 0.0;
+    }
+    const uint32_t x = __ldg(col + a) - lo;  // wraps past L for remote slots
+    if (x < L) uf_union(parent, key, u, x);
+    return 0.0;
   }
-  return false;
+};
+
+struct NoFinishPart {
+  __device__ __forceinline__ void operator()(uint32_t, double) const {}
+};
+
+// Afforest's first pass over the local arcs: every slot united with the local ones among its
+// first k arcs (the hubs, on a relabelled graph)
+__global__ void k_pcc_sample(uint64_t L, const uint64_t* __restrict__ off, const uint32_t* __restrict__ col, uint32_t k,
+                             uint32_t lo, uint32_t* parent, const uint32_t* __restrict__ key) {
+  for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < L; u += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t a0 = off[u], a1 = off[u + 1];
+    for (uint64_t a = a0; a < a1 && a < a0 + k; ++a) {
+      const uint32_t x = __ldg(col + a) - lo;
+      if (x < L) uf_union(parent, key, (uint32_t)u, x);
+    }
+  }
 }
 
-// CC, one superstep over the rows of one degree bin, G lanes per row (bins 0-5 of the row
-// schedule): the smallest label among the row's neighbours (labels of all slots from the
-// previous superstep), then cc_update.
+// arcs of the rows that lead to another rank's slots
+__global__ void k_pcc_count_remote(uint64_t arcs, const uint32_t* __restrict__ col, uint32_t lo, uint32_t L,
+                                   unsigned long long* __restrict__ out) {
+  unsigned long long c = 0;
+  for (uint64_t a = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; a < arcs; a += (uint64_t)gridDim.x * blockDim.x)
+    c += (uint32_t)(__ldg(col + a) - lo) >= L;
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31u) == 0 && c) atomicAdd(out, c);
+}
+
+// after phase 1 (parent[i] = root of i): every slot's label is its root's key, every root's
+// component label too
+__global__ void k_pcc_labels(uint64_t L, const uint32_t* __restrict__ parent, const uint32_t* __restrict__ key,
+                             uint32_t* __restrict__ lab, uint32_t* __restrict__ rootlab) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < L; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t r = parent[i];
+    lab[i] = key[r];
+    if (r == i) rootlab[i] = key[i];
+  }
+}
+
+// CC, phase 2 (one round): the smallest label behind the row's remote arcs (labels of all slots
+// from the round's all-gather) offered to the row's local component.  G lanes per row.
 template <int G>
-__global__ void __launch_bounds__(256) k_part_cc_lanes(const uint32_t* __restrict__ rows, uint64_t count,
+__global__ void __launch_bounds__(256) k_pcc_cut_lanes(const uint32_t* __restrict__ rows, uint64_t count,
                                                        const uint64_t* __restrict__ off, const uint32_t* __restrict__ col,
-                                                       const uint32_t* __restrict__ lab_all, const uint32_t* __restrict__ xof,
-                                                       uint32_t* __restrict__ lab, BfsCounters* __restrict__ c) {
+                                                       uint32_t lo, uint32_t L, const uint32_t* __restrict__ lab_all,
+                                                       const uint32_t* __restrict__ parent, uint32_t* __restrict__ rootlab) {
   const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   const uint32_t lig = threadIdx.x % G;
   const uint64_t ngroups = ((uint64_t)gridDim.x * blockDim.x) / G;
-  unsigned long long changed = 0;
   // warp-uniform trip count: every lane takes part in the shuffles
   for (uint64_t base = (tid / G) & ~(uint64_t)(32 / G - 1); base < count; base += ngroups) {
     const uint64_t r = base + (threadIdx.x & 31u) / G;
     uint32_t m = 0xffffffffu, v = 0;
     if (r < count) {
       v = rows[r];
-      for (uint64_t a = off[v] + lig; a < off[v + 1]; a += G) m = min(m, lab_all[__ldg(col + a)]);
+      for (uint64_t a = off[v] + lig; a < off[v + 1]; a += G) {
+        const uint32_t x = __ldg(col + a);
+        if (x - lo >= L) m = min(m, lab_all[x]);
+      }
     }
 #pragma unroll
     for (int o = G / 2; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (r < count && lig == 0 && cc_update(v, m, lab_all, xof, lab)) ++changed;
+    if (r < count && lig == 0 && m != 0xffffffffu) {
+      const uint32_t root = parent[v];
+      if (m < rootlab[root]) atomicMin(rootlab + root, m);
+    }
   }
-  if (changed) atomicAdd(&c->next_count, changed);
 }
 
-// CC for the long rows (bins 6-7): CTA per row.
-__global__ void __launch_bounds__(256) k_part_cc_rows(const uint32_t* __restrict__ rows, uint64_t count,
+// the same for the long rows (bins 6-7): CTA per row
+__global__ void __launch_bounds__(256) k_pcc_cut_rows(const uint32_t* __restrict__ rows, uint64_t count,
                                                       const uint64_t* __restrict__ off, const uint32_t* __restrict__ col,
-                                                      const uint32_t* __restrict__ lab_all, const uint32_t* __restrict__ xof,
-                                                      uint32_t* __restrict__ lab, BfsCounters* __restrict__ c) {
-  __shared__ uint32_t s_min[8];
-  const uint32_t lane = threadIdx.x & 31u;
-  unsigned long long changed = 0;
+                                                      uint32_t lo, uint32_t L, const uint32_t* __restrict__ lab_all,
+                                                      const uint32_t* __restrict__ parent, uint32_t* __restrict__ rootlab) {
   for (uint64_t r = blockIdx.x; r < count; r += gridDim.x) {
     const uint32_t v = rows[r];
     uint32_t m = 0xffffffffu;
-    for (uint64_t a = off[v] + threadIdx.x; a < off[v + 1]; a += blockDim.x) m = min(m, lab_all[__ldg(col + a)]);
-    m = __reduce_min_sync(0xffffffffu, m);
-    if (lane == 0) s_min[threadIdx.x >> 5] = m;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-      m = threadIdx.x < (blockDim.x >> 5) ? s_min[threadIdx.x] : 0xffffffffu;
-      m = __reduce_min_sync(0xffffffffu, m);
+    for (uint64_t a = off[v] + threadIdx.x; a < off[v + 1]; a += blockDim.x) {
+      const uint32_t x = __ldg(col + a);
+      if (x - lo >= L) m = min(m, lab_all[x]);
     }
-    __syncthreads();
-    if (threadIdx.x == 0 && cc_update(v, m, lab_all, xof, lab)) ++changed;
+    m = __reduce_min_sync(0xffffffffu, m);
+    if ((threadIdx.x & 31u) == 0 && m != 0xffffffffu) {
+      const uint32_t root = parent[v];
+      if (m < rootlab[root]) atomicMin(rootlab + root, m);
+    }
   }
-  if (changed) atomicAdd(&c->next_count, changed);
+}
+
+// roots: the shortcut through the vertex the label names (its label in the round's snapshot)
+__global__ void k_pcc_roots(uint64_t L, const uint32_t* __restrict__ parent, const uint32_t* __restrict__ lab_all,
+                            const uint32_t* __restrict__ xof, uint32_t* __restrict__ rootlab) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < L; i += (uint64_t)gridDim.x * blockDim.x) {
+    if (parent[i] != i) continue;
+    const uint32_t l = rootlab[i];
+    if (l == 0xffffffffu) continue;  // padding
+    const uint32_t s = lab_all[xof[l]];
+    if (s < l) rootlab[i] = s;
+  }
+}
+
+// members take their component's label; c->next_count += slots whose label dropped
+__global__ void k_pcc_members(uint64_t L, const uint32_t* __restrict__ parent, const uint32_t* __restrict__ rootlab,
+                              uint32_t* __restrict__ lab, BfsCounters* __restrict__ c) {
+  unsigned long long changed = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < L; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t l = rootlab[parent[i]];
+    if (l < lab[i]) {
+      lab[i] = l;
+      ++changed;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) changed += __shfl_xor_sync(0xffffffffu, changed, o);
+  if ((threadIdx.x & 31u) == 0 && changed) atomicAdd(&c->next_count, changed);
 }
 
 // Rows of slots [0, L) of rank p from (off, col): *loff (L + 1) and *lcol allocated here.
@@ -911,59 +987,113 @@ int gre_part_cc(gre_part p, uint32_t* label, gre_exchange_fn xchg, void* ctx, gr
   GRE_CHECK(use_graph(s));
   stats_reset(st);
   const uint64_t n = p->n, P = p->nparts, L = p->L, me = p->rank;
-  uint32_t *lab, *lab_all, *dout;
+  const uint32_t lo = (uint32_t)(me * L);
+  const bool sym = s->roff == s->off;
+  const uint32_t* key = p->xmap + me * L;  // caller id of every owned slot (padding: 0xffffffff)
+  uint32_t *lab, *lab_all, *dout, *parent, *rootlab, *skip;
+  double* partial;
   BfsCounters *c, *call;
+  constexpr uint32_t kSampled = 2, kSample = 1024;
   GRE_CHECK(ws_array(s, WS_A, L, &lab));
   GRE_CHECK(ws_array(s, WS_B, P * L, &lab_all));
-  GRE_CHECK(ws_array(s, WS_COUNTERS, 1, &c));
+  GRE_CHECK(ws_array(s, WS_C, L, &parent));
+  GRE_CHECK(ws_array(s, WS_D, L, &rootlab));
+  GRE_CHECK(ws_array(s, WS_E, ((L + 31) >> 5) + kSample, &skip));
+  GRE_CHECK(ws_array(s, WS_F, std::max(s->bins_in.n_hub_chunks, s->bins_out.n_hub_chunks) + 1, &partial));
+  GRE_CHECK(ws_array(s, WS_COUNTERS, 2, &c));
   GRE_CHECK(ws_array(s, WS_OUTBUF2, P, &call));
   GRE_CHECK(prepare_output(s, label, n, WS_OUTBUF, &dout));
+  unsigned long long* counts = (unsigned long long*)(c + 1);  // Afforest's arc counts (byte model)
+  uint32_t* sample = skip + ((L + 31) >> 5);
+  if (p->cc_remote == ~0ull) {  // once per part: arcs that cross to other ranks
+    GRE_CUDA(cudaMemsetAsync(counts, 0, sizeof(unsigned long long), s->stream));
+    k_pcc_count_remote<<<grid_for(p->arcs_in, 256, 8), 256, 0, s->stream>>>(p->arcs_in, s->rcol, lo, (uint32_t)L, counts);
+    if (!sym) k_pcc_count_remote<<<grid_for(p->arcs_out, 256, 8), 256, 0, s->stream>>>(p->arcs_out, s->col, lo, (uint32_t)L, counts);
+    GRE_LAUNCH_CHECK();
+    unsigned long long h = 0;
+    GRE_CUDA(cudaMemcpyAsync(&h, counts, sizeof h, cudaMemcpyDeviceToHost, s->stream));
+    GRE_CUDA(cudaStreamSynchronize(s->stream));
+    p->cc_remote = h;
+  }
   RunTimer timer(s);
-  k_part_cc_init<<<grid_for(L, 256), 256, 0, s->stream>>>(L, p->xmap + me * L, lab);
+  // phase 1: union-find over the arcs inside this rank (Afforest on a symmetric graph, as gre_cc:
+  // the first arcs of every row, then the rows outside the largest local component)
+  uint64_t visited = 0;
+  k_uf_init<<<grid_for(L, 256), 256, 0, s->stream>>>(L, parent);
+  if (sym) {
+    k_pcc_sample<<<grid_for(L, 256), 256, 0, s->stream>>>(L, s->roff, s->rcol, kSampled, lo, parent, key);
+    const uint64_t stride = L > kSample ? L / kSample : 1;
+    const uint32_t ns = (uint32_t)std::min<uint64_t>(kSample, (L + stride - 1) / stride);
+    k_uf_compress<<<grid_for(L, 256), 256, 0, s->stream>>>(L, parent, stride, sample, ns);
+    std::vector<uint32_t> hs(kSample, 0);
+    GRE_CUDA(cudaMemcpyAsync(hs.data(), sample, sizeof(uint32_t) * ns, cudaMemcpyDeviceToHost, s->stream));
+    GRE_CUDA(cudaStreamSynchronize(s->stream));
+    const uint32_t big = uf_most_frequent(hs, ns);
+    GRE_CUDA(cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), s->stream));
+    k_uf_skipbits<<<grid_for((L + 31) >> 5, 256), 256, 0, s->stream>>>(L, parent, s->roff, big, kSampled, skip, counts);
+    HookLocal rest{s->rcol, parent, key, lo, (uint32_t)L, skip, s->roff, kSampled};
+    GRE_CHECK(rows::reduce_rows(s->bins_in, s->roff, rest, NoFinishPart{}, partial, s->stream));
+    unsigned long long h[2] = {0, 0};
+    GRE_CUDA(cudaMemcpyAsync(h, counts, sizeof h, cudaMemcpyDeviceToHost, s->stream));
+    GRE_CUDA(cudaStreamSynchronize(s->stream));
+    visited = h[0] + h[1];
+  } else {  // weak components: in-arcs and out-arcs
+    GRE_CHECK(rows::reduce_rows(s->bins_in, s->roff, HookLocal{s->rcol, parent, key, lo, (uint32_t)L}, NoFinishPart{}, partial,
+                                s->stream));
+    GRE_CHECK(rows::reduce_rows(s->bins_out, s->off, HookLocal{s->col, parent, key, lo, (uint32_t)L}, NoFinishPart{}, partial,
+                                s->stream));
+    visited = p->arcs_in + p->arcs_out;
+  }
+  k_uf_compress<<<grid_for(L, 256), 256, 0, s->stream>>>(L, parent, L + 1, nullptr, 0);
+  k_pcc_labels<<<grid_for(L, 256), 256, 0, s->stream>>>(L, parent, key, lab, rootlab);
   GRE_LAUNCH_CHECK();
-  // label propagation to the smallest caller id with shortcuts (min over in-arcs, and over
-  // out-arcs too on a directed graph: weak components, as gre_cc); rows split by the degree bins
-  // (bins 0-5 one to 32 lanes per row, 6-7 CTA per row)
-  auto sweep = [&](const DegreeBins& B, const uint64_t* off, const uint32_t* col) {
-    const uint64_t nbig = B.count[6] + B.count[7];
+  uint64_t bytes = 8 * (L + 1) + 12 * visited + 16 * L;
+  // phase 2: the local components' labels meet over the cut arcs, a round per all-gather of the
+  // labels; each round also takes the shortcut through the vertex a label names.  Every rank
+  // takes the same collectives (a rank without cut arcs still exchanges).
+  auto cut_sweep = [&](const DegreeBins& B, const uint64_t* off, const uint32_t* col) {
     auto lanes = [&](auto kernel, int b, int G) {
       if (B.count[b])
-        kernel<<<grid_for(B.count[b] * G, 256, 8), 256, 0, s->stream>>>(B.rows + B.start[b], B.count[b], off, col, lab_all, p->xof,
-                                                                          lab, c);
+        kernel<<<grid_for(B.count[b] * G, 256, 8), 256, 0, s->stream>>>(B.rows + B.start[b], B.count[b], off, col, lo,
+                                                                          (uint32_t)L, lab_all, parent, rootlab);
     };
-    lanes(k_part_cc_lanes<1>, 0, 1);
-    lanes(k_part_cc_lanes<2>, 1, 2);
-    lanes(k_part_cc_lanes<4>, 2, 4);
-    lanes(k_part_cc_lanes<8>, 3, 8);
-    lanes(k_part_cc_lanes<16>, 4, 16);
-    lanes(k_part_cc_lanes<32>, 5, 32);
+    lanes(k_pcc_cut_lanes<1>, 0, 1);
+    lanes(k_pcc_cut_lanes<2>, 1, 2);
+    lanes(k_pcc_cut_lanes<4>, 2, 4);
+    lanes(k_pcc_cut_lanes<8>, 3, 8);
+    lanes(k_pcc_cut_lanes<16>, 4, 16);
+    lanes(k_pcc_cut_lanes<32>, 5, 32);
+    const uint64_t nbig = B.count[6] + B.count[7];
     if (nbig)
-      k_part_cc_rows<<<grid_for(nbig * 256, 256, 8), 256, 0, s->stream>>>(B.rows + B.start[6], nbig, off, col, lab_all, p->xof,
-                                                                            lab, c);
+      k_pcc_cut_rows<<<grid_for(nbig * 256, 256, 8), 256, 0, s->stream>>>(B.rows + B.start[6], nbig, off, col, lo, (uint32_t)L,
+                                                                            lab_all, parent, rootlab);
   };
   uint32_t steps = 0;
-  uint64_t bytes = 0;
   BfsCounters sum;
   for (;;) {
     GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLGATHER, lab, lab_all, 4 * L));
     GRE_CUDA(cudaMemsetAsync(c, 0, sizeof(BfsCounters), s->stream));
-    sweep(s->bins_in, s->roff, s->rcol);
-    if (s->roff != s->off) sweep(s->bins_out, s->off, s->col);
+    if (p->cc_remote) {
+      cut_sweep(s->bins_in, s->roff, s->rcol);
+      if (!sym) cut_sweep(s->bins_out, s->off, s->col);
+      bytes += 4 * (p->arcs_in + (sym ? 0 : p->arcs_out)) + 4 * p->cc_remote;
+    }
+    k_pcc_roots<<<grid_for(L, 256), 256, 0, s->stream>>>(L, parent, lab_all, p->xof, rootlab);
+    k_pcc_members<<<grid_for(L, 256), 256, 0, s->stream>>>(L, parent, rootlab, lab, c);
     GRE_LAUNCH_CHECK();
     GRE_CHECK(exchange_counters(p, xchg, ctx, c, call, &sum, nullptr));
     ++steps;
-    bytes += 8 * (L + 1) + 8 * (p->arcs_in + (s->roff != s->off ? p->arcs_out : 0)) + 4 * P * L + 8 * L;
+    bytes += 4 * P * L + 16 * L;
     stats_record(st, sum.next_count);
     if (sum.next_count == 0) break;
   }
-  GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLGATHER, lab, lab_all, 4 * L));
   k_part_out<uint32_t><<<grid_for(P * L, 256), 256, 0, s->stream>>>(P * L, p->xmap, lab_all, dout);
   GRE_LAUNCH_CHECK();
   GRE_CHECK(finish_output(s, label, dout, n));
   GRE_CHECK(timer.stop(st));
   if (st) {
     st->supersteps = steps;
-    st->arcs_traversed = (p->arcs_in + (s->roff != s->off ? p->arcs_out : 0)) * (uint64_t)steps;
+    st->arcs_traversed = visited + (uint64_t)steps * (p->cc_remote ? p->arcs_in + (sym ? 0 : p->arcs_out) : 0);
     st->traversed_edges = s->symmetric() ? p->m / 2 : p->m;
     st->algo_bytes = bytes;
   }

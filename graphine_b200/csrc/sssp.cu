@@ -334,6 +334,173 @@ static int relax_binned(const DegreeBins& B, const RelaxRange& R, cudaStream_t s
   return GRE_SUCCESS;
 }
 
+// Pull form of a large pass (direction-optimising, as bottom-up BFS): instead of the frontier
+// pushing along its arcs, every vertex that can still improve scans its own light (or heavy)
+// arcs for neighbours in the frontier bitmap and takes the smallest dist[u] + w.  Valid when the
+// graph is symmetric and w(u->v) == w(v->u) (g->w32_symmetric): v's arc to u then carries the
+// weight, and the light/heavy class, of u's arc to v, so the candidate values are exactly those
+// the push would offer.  What it saves: the push's reads and atomics land on the heads, spread
+// over all of dist (DRAM); the pull reads dist only at frontier vertices (on RMAT mostly the
+// hubs, which the degree-ordered ids keep in L2) and writes each improved vertex once.  Rows
+// whose distance is below `lo` are settled (every earlier bucket is final) and are skipped
+// after one read of dist.
+struct PullRange {
+  const uint32_t* __restrict__ front;  // sources: the near frontier (light pass) or the bucket (heavy pass)
+  const uint64_t* __restrict__ off;
+  const uint64_t* __restrict__ lend;
+  const uint32_t* __restrict__ col;
+  const uint32_t* __restrict__ w;
+  uint32_t* __restrict__ dist;
+  uint32_t* __restrict__ changed;
+  unsigned long long* __restrict__ counts;  // [0] arcs scanned, [1] frontier hits
+  bool heavy;
+  uint32_t lo;
+  __device__ __forceinline__ void range(uint32_t v, uint64_t* a0, uint64_t* a1) const {
+    *a0 = heavy ? lend[v] : off[v];
+    *a1 = heavy ? off[v + 1] : lend[v];
+  }
+  // smallest dist[u] + w over the arcs a, a + step, ... < hi whose tail u is in the frontier;
+  // four column loads and bit tests in flight, then the hits' weights and distances
+  __device__ __forceinline__ uint32_t best(uint64_t a, uint64_t hi, uint64_t step, unsigned long long* hits) const {
+    uint32_t b = 0xffffffffu;
+    for (; a + 3 * step < hi; a += 4 * step) {
+      uint32_t u[4];
+      bool in[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) u[k] = __ldg(col + a + k * step);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) in[k] = (__ldg(front + (u[k] >> 5)) >> (u[k] & 31u)) & 1u;
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (in[k]) {
+          const uint32_t nd = __ldcg(dist + u[k]) + __ldg(w + a + k * step);
+          b = nd < b ? nd : b;
+          ++*hits;
+        }
+    }
+    for (; a < hi; a += step) {
+      const uint32_t u = __ldg(col + a);
+      if ((__ldg(front + (u >> 5)) >> (u & 31u)) & 1u) {
+        const uint32_t nd = __ldcg(dist + u) + __ldg(w + a);
+        b = nd < b ? nd : b;
+        ++*hits;
+      }
+    }
+    return b;
+  }
+  __device__ __forceinline__ void improve(uint32_t v, uint32_t dv, uint32_t b) const {
+    if (b < dv) {
+      atomicMin(dist + v, b);
+      atomicOr(changed + (v >> 5), 1u << (v & 31u));
+    }
+  }
+};
+
+__device__ __forceinline__ void add_counts(unsigned long long* c, unsigned long long scanned, unsigned long long hits) {
+  for (int o = 16; o > 0; o >>= 1) {
+    scanned += __shfl_xor_sync(0xffffffffu, scanned, o);
+    hits += __shfl_xor_sync(0xffffffffu, hits, o);
+  }
+  if ((threadIdx.x & 31u) == 0) {
+    if (scanned) atomicAdd(c, scanned);
+    if (hits) atomicAdd(c + 1, hits);
+  }
+}
+
+// G lanes per row; the group's lanes share the row, so they take every branch together and the
+// group minimum is a shuffle over the group's own lanes
+template <int G>
+__global__ void __launch_bounds__(256) k_pull_lanes(const uint32_t* __restrict__ rows, uint64_t count, PullRange R) {
+  const uint32_t lane = threadIdx.x & 31u, lig = lane % G;
+  const unsigned gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << (lane - lig));
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned long long scanned = 0, hits = 0;
+  for (uint64_t base = warp * (32 / G); base < count; base += nwarps * (32 / G)) {
+    const uint64_t i = base + lane / G;
+    if (i >= count) continue;
+    const uint32_t v = rows[i];
+    const uint32_t dv = __ldcg(R.dist + v);
+    if (dv < R.lo) continue;
+    uint64_t a0, a1;
+    R.range(v, &a0, &a1);
+    if (a0 >= a1) continue;
+    if (lig == 0) scanned += a1 - a0;
+    uint32_t b = R.best(a0 + lig, a1, G, &hits);
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) {
+      const uint32_t x = __shfl_xor_sync(gmask, b, o);
+      b = x < b ? x : b;
+    }
+    if (lig == 0) R.improve(v, dv, b);
+  }
+  add_counts(R.counts, scanned, hits);
+}
+
+__device__ __forceinline__ uint32_t warp_min(uint32_t b) {
+  for (int o = 16; o > 0; o >>= 1) {
+    const uint32_t x = __shfl_xor_sync(0xffffffffu, b, o);
+    b = x < b ? x : b;
+  }
+  return b;
+}
+
+// a CTA per row; each warp offers its own minimum (at most 8 atomics per improved row)
+__global__ void __launch_bounds__(256) k_pull_cta(const uint32_t* __restrict__ rows, uint64_t count, PullRange R) {
+  unsigned long long scanned = 0, hits = 0;
+  for (uint64_t i = blockIdx.x; i < count; i += gridDim.x) {
+    const uint32_t v = rows[i];
+    const uint32_t dv = __ldcg(R.dist + v);
+    if (dv < R.lo) continue;
+    uint64_t a0, a1;
+    R.range(v, &a0, &a1);
+    if (a0 >= a1) continue;
+    if (threadIdx.x == 0) scanned += a1 - a0;
+    const uint32_t b = warp_min(R.best(a0 + threadIdx.x, a1, blockDim.x, &hits));
+    if ((threadIdx.x & 31u) == 0) R.improve(v, dv, b);
+  }
+  add_counts(R.counts, scanned, hits);
+}
+
+// a CTA per 65536-arc chunk of the longest rows, cut to the light or heavy range
+__global__ void __launch_bounds__(256) k_pull_chunks(const uint32_t* __restrict__ rows, const uint64_t* __restrict__ chunk_row,
+                                                     const uint64_t* __restrict__ chunk_begin, uint64_t nchunks, uint64_t chunk,
+                                                     PullRange R) {
+  unsigned long long scanned = 0, hits = 0;
+  for (uint64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    const uint32_t v = rows[chunk_row[c]];
+    const uint32_t dv = __ldcg(R.dist + v);
+    if (dv < R.lo) continue;
+    uint64_t a0, a1;
+    R.range(v, &a0, &a1);
+    const uint64_t c0 = chunk_begin[c], c1 = c0 + chunk;
+    a0 = a0 > c0 ? a0 : c0;
+    a1 = a1 < c1 ? a1 : c1;
+    if (a0 >= a1) continue;
+    if (threadIdx.x == 0) scanned += a1 - a0;
+    const uint32_t b = warp_min(R.best(a0 + threadIdx.x, a1, blockDim.x, &hits));
+    if ((threadIdx.x & 31u) == 0) R.improve(v, dv, b);
+  }
+  add_counts(R.counts, scanned, hits);
+}
+
+static int pull_binned(const DegreeBins& B, const PullRange& R, cudaStream_t s) {
+  const uint32_t* r = B.rows;
+  auto grid = [](uint64_t threads) { return grid_for(threads, 256, 8); };
+  if (B.count[0]) k_pull_lanes<1><<<grid(B.count[0]), 256, 0, s>>>(r + B.start[0], B.count[0], R);
+  if (B.count[1]) k_pull_lanes<2><<<grid(B.count[1] * 2), 256, 0, s>>>(r + B.start[1], B.count[1], R);
+  if (B.count[2]) k_pull_lanes<4><<<grid(B.count[2] * 4), 256, 0, s>>>(r + B.start[2], B.count[2], R);
+  if (B.count[3]) k_pull_lanes<8><<<grid(B.count[3] * 8), 256, 0, s>>>(r + B.start[3], B.count[3], R);
+  if (B.count[4]) k_pull_lanes<16><<<grid(B.count[4] * 16), 256, 0, s>>>(r + B.start[4], B.count[4], R);
+  if (B.count[5]) k_pull_lanes<32><<<grid(B.count[5] * 32), 256, 0, s>>>(r + B.start[5], B.count[5], R);
+  if (B.count[6]) k_pull_cta<<<grid(B.count[6] * 256), 256, 0, s>>>(r + B.start[6], B.count[6], R);
+  if (B.count[7])
+    k_pull_chunks<<<grid(B.n_hub_chunks * 256), 256, 0, s>>>(r + B.start[7], B.hub_chunk_row, B.hub_chunk_begin, B.n_hub_chunks,
+                                                            B.sched.hub_chunk, R);
+  GRE_LAUNCH_CHECK();
+  return GRE_SUCCESS;
+}
+
 // Which vertices have light arcs ([off, lend) non-empty) and which heavy ones ([lend, off+1)):
 // one bit each, so that the passes below test a word instead of reading three offsets per vertex.
 __global__ void k_sssp_classes(uint64_t n, const uint64_t* __restrict__ off, const uint64_t* __restrict__ lend,
@@ -540,6 +707,14 @@ static uint64_t binned_frontier() {
   return 64;
 }
 
+// Whether those large passes pull (over the vertices that can still improve) instead of pushing
+// (along the frontier's arcs), where the weights allow it (g->w32_symmetric).  Default on; the
+// GRE_SSSP_PULL environment variable set to 0 keeps the push form.
+static bool pull_enabled() {
+  if (const char* e = getenv("GRE_SSSP_PULL")) return strtoul(e, nullptr, 10) != 0;
+  return true;
+}
+
 // The relaxation of one frontier pass: tile starts, then k_sssp_relax over one wave of CTAs.
 int sssp_relax_tiles(cudaStream_t stream, const uint32_t* queue, uint64_t nq, const uint64_t* prefix, uint64_t total,
                      uint32_t* tstart, const uint64_t* base, const uint32_t* col, const uint32_t* w, const uint32_t* srcdist,
@@ -609,8 +784,11 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
   uint32_t *lbits, *hbits;
   GRE_CHECK(ws_array(g, WS_SSSP_L, nwords, &lbits));
   GRE_CHECK(ws_array(g, WS_SSSP_H, nwords, &hbits));
-  GRE_CHECK(ws_array(g, WS_COUNTERS, 10, &cnt));  // 8 uint32 counters, then the binned passes' arc count
+  // 8 uint32 counters, then the binned passes' arc count and the pull passes' scanned arcs and hits
+  GRE_CHECK(ws_array(g, WS_COUNTERS, 14, &cnt));
   unsigned long long* binned_arcs = (unsigned long long*)(cnt + 8);
+  unsigned long long* pull_counts = (unsigned long long*)(cnt + 10);
+  const bool pull = g->w32_symmetric && pull_enabled();
   // large frontiers go through the degree bins of the CSR (the symmetric CSC is the CSR)
   const bool sym = g->symmetric();
   GRE_CHECK(ensure_bins(g, sym));
@@ -624,7 +802,7 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
   GRE_CUDA(cudaMemsetAsync(changed, 0, sizeof(uint32_t) * nwords, g->stream));
   GRE_CUDA(cudaMemsetAsync(infar, 0, sizeof(uint32_t) * nwords, g->stream));
   GRE_CUDA(cudaMemsetAsync(inbucket, 0, sizeof(uint32_t) * nwords, g->stream));
-  GRE_CUDA(cudaMemsetAsync(binned_arcs, 0, sizeof(unsigned long long), g->stream));
+  GRE_CUDA(cudaMemsetAsync(binned_arcs, 0, 3 * sizeof(unsigned long long), g->stream));
   k_sssp_classes<<<grid_for(n, 256, 8), 256, 0, g->stream>>>(n, off, lend, lbits, hbits);
   uint32_t limit = delta ? delta : 0xffffffffu;
   uint64_t nq = 0, nfar = 0, nb = 0, relaxed = 0, bytes = 0;
@@ -662,8 +840,17 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
         k_queue_to_bits<<<grid_for(nlist, 256), 256, 0, g->stream>>>(list, nlist, front);
       }
       GRE_CHECK(init_counters(g, cnt, 0, (uint32_t)nfar, (uint32_t)nb));
-      RelaxRange R{front, off, lend, col, w, dist, changed, binned_arcs, heavy, nullptr};
-      GRE_CHECK(relax_binned<false>(bins, R, g->stream));
+      if (pull) {
+        // light pass: every vertex outside the settled buckets may improve; heavy pass: only
+        // vertices at or above the limit (heavy arcs from the bucket land there)
+        const uint32_t lo = heavy ? limit : (limit > delta ? limit - delta : 0u);
+        PullRange P{front, off, lend, col, w, dist, changed, pull_counts, heavy, lo};
+        GRE_CHECK(pull_binned(bins, P, g->stream));
+        bytes += 16 * n;  // per row: its id, distance and range bounds (arcs at the end)
+      } else {
+        RelaxRange R{front, off, lend, col, w, dist, changed, binned_arcs, heavy, nullptr};
+        GRE_CHECK(relax_binned<false>(bins, R, g->stream));
+      }
       k_sssp_classify<<<grid_for(nwords, 256, 8), 256, 0, g->stream>>>(nwords, changed, dist, lbits, hbits, limit, out_near, infar,
                                                                         far, inbucket, blist, cnt);
       GRE_LAUNCH_CHECK();
@@ -743,11 +930,12 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
       std::swap(far, far2);
     }
   }
-  unsigned long long barcs = 0;
-  GRE_CUDA(cudaMemcpyAsync(&barcs, binned_arcs, sizeof barcs, cudaMemcpyDeviceToHost, g->stream));
+  unsigned long long bc[3] = {0, 0, 0};
+  GRE_CUDA(cudaMemcpyAsync(bc, binned_arcs, sizeof bc, cudaMemcpyDeviceToHost, g->stream));
   GRE_CUDA(cudaStreamSynchronize(g->stream));
-  relaxed += barcs;
-  bytes += 12 * barcs;  // column + weight + distance probe per arc
+  relaxed += bc[0] + bc[1];
+  bytes += 12 * bc[0];              // push: column + weight + distance probe per arc
+  bytes += 4 * bc[1] + 8 * bc[2];   // pull: column per arc scanned (+ L2-held bitmap), weight + distance per hit
   if (st) {
     st->supersteps += steps ? steps - 1 : 0;
     st->arcs_traversed += relaxed;

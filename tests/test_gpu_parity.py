@@ -513,10 +513,13 @@ def test_s20_cc_properties(rmat20):
     np.testing.assert_array_equal(lab, lab2)
 
 
+@pytest.mark.parametrize("pull", ["0", "1"], ids=["push", "pull"])
 @pytest.mark.parametrize("binned", ["0", "4294967296", "64"], ids=["tiles", "bins", "default"])
-def test_sssp_relaxation_forms_agree(monkeypatch, binned):
-    """Arc tiles only, degree bins only, and the default mix give the oracle's distances."""
+def test_sssp_relaxation_forms_agree(monkeypatch, binned, pull):
+    """Arc tiles only, degree bins only (every pass, pushed along the frontier's arcs or pulled
+    by the vertices that can improve), and the default mix give the oracle's distances."""
     monkeypatch.setenv("GRE_SSSP_BINNED", binned)
+    monkeypatch.setenv("GRE_SSSP_PULL", pull)
     for sym in (True, False):
         n, off, col = G.rmat_host(12, 16, 9, sym)
         g = G.Graph.from_csr(n, off, col, dir=G.InOut if sym else G.Out, symmetric=sym, reorder=True)
@@ -543,3 +546,24 @@ def test_plugin_output_statistics(golden, name, reorder):
     assert st.plugin_count == int(np.sum(case["cc_label"] == np.arange(int(case["n"]))))
     _, st = G.cc(g)  # the fast paths run no plugin
     assert st.plugin_count == 0 and st.plugin_value == 0.0
+
+
+@pytest.mark.parametrize("pull", ["0", "1"], ids=["push", "pull"])
+def test_sssp_pull_needs_symmetric_weights(monkeypatch, pull):
+    """The pull form reads w(v->u) for the arc u->v: it runs only where the weights are a function
+    of the undirected edge (hash weights), and explicit per-arc weights that differ between the two
+    directions still give the oracle's distances (push form) with every pass through the bins."""
+    monkeypatch.setenv("GRE_SSSP_PULL", pull)
+    monkeypatch.setenv("GRE_SSSP_BINNED", "4294967296")  # every pass through the bins
+    n, off, col = G.rmat_host(13, 16, 5, True)
+    R = O.Restatement.from_csr(n, off, col)
+    roots = G.sample_sources(off, 4, 2)
+    g = G.Graph.from_csr(n, off, col, dir=G.InOut, symmetric=True, reorder=True)
+    w = np.random.default_rng(9).integers(1, 256, len(col)).astype(np.uint32)  # not symmetric
+    g.loadEdgeProperty(w)
+    np.testing.assert_array_equal(G.sssp(g, roots)[0].reshape(len(roots), n), R.sssp_many(roots, 0, w))
+    g.set_weights_hash(4)
+    np.testing.assert_array_equal(G.sssp(g, roots)[0].reshape(len(roots), n), R.sssp_many(roots, 4))
+    for d in ("0", "1", "300"):  # Bellman-Ford frontier, unit buckets, one bucket holding everything
+        monkeypatch.setenv("GRE_SSSP_DELTA", d)
+        np.testing.assert_array_equal(G.sssp(g, roots)[0].reshape(len(roots), n), R.sssp_many(roots, 4))
