@@ -495,6 +495,7 @@ static int bc_batched(gre_graph g, const std::vector<uint32_t>& hs, double* dbc,
     k_bcm_seed<<<1, 32, 0, g->stream>>>(srcs, k, seen, (unsigned long long*)g->bc_fpool, sigma);
     // forward: frontier words of every level
     uint64_t nl = 1;  // levels stored: F_0 .. F_{nl-1}
+    unsigned long long live = full;  // sources whose frontier is not empty
     while (true) {
       GRE_CHECK(fpool_levels(g, nl + 1));
       unsigned long long* fd = (unsigned long long*)g->bc_fpool + (nl - 1) * n;
@@ -502,7 +503,7 @@ static int bc_batched(gre_graph g, const std::vector<uint32_t>& hs, double* dbc,
       // push from a sparse frontier, pull otherwise (same frontier words either way)
       GRE_CUDA(cudaMemsetAsync(cnt, 0, 64, g->stream));
       ms::k_frontier_list<<<grid_for(n, 256, 8), 256, 0, g->stream>>>(n, fd, g->off, list, (unsigned int*)(cnt + 2), cnt + 3);
-      unsigned long long h[5];
+      unsigned long long h[6];
       GRE_CUDA(cudaMemcpyAsync(h, cnt, sizeof(unsigned long long) * 4, cudaMemcpyDeviceToHost, g->stream));
       GRE_CUDA(cudaStreamSynchronize(g->stream));
       const bool push = h[3] * 14 < g->m;
@@ -510,8 +511,8 @@ static int bc_batched(gre_graph g, const std::vector<uint32_t>& hs, double* dbc,
         ms::k_push<<<grid_for((h[2] & 0xffffffffull) * 32, 256, 8), 256, 0, g->stream>>>(list, (unsigned int*)(cnt + 2), g->off,
                                                                                           g->col, fd, seen, acc);
       else
-        GRE_CHECK(ms::pull(g->bins_in, full, g->roff, g->rcol, fd, seen, acc, cnt + 4, g->stream));
-      ms::k_commit<<<grid_for(n, 256, 8), 256, 0, g->stream>>>(n, acc, seen, fn, nullptr, 0, cnt);
+        GRE_CHECK(ms::pull(g->bins_in, live, g->roff, g->rcol, fd, seen, acc, cnt + 4, g->stream));
+      ms::k_commit<<<grid_for(n, 256, 8), 256, 0, g->stream>>>(n, acc, seen, fn, nullptr, 0, cnt, cnt + 5);
       GRE_LAUNCH_CHECK();
       GRE_CUDA(cudaMemcpyAsync(h, cnt, sizeof h, cudaMemcpyDeviceToHost, g->stream));
       GRE_CUDA(cudaStreamSynchronize(g->stream));
@@ -523,6 +524,7 @@ static int bc_batched(gre_graph g, const std::vector<uint32_t>& hs, double* dbc,
         bytes += 24 * n + 12 * h[4];
       }
       if (h[0] == 0) break;
+      live = h[5];
       ++nl;
     }
     unsigned long long* F = (unsigned long long*)g->bc_fpool;

@@ -473,11 +473,12 @@ int gre_msbfs(gre_graph g, const uint32_t* srcs, uint32_t nsrc, int32_t* levels,
     k_ms_seed<<<1, 32, 0, g->stream>>>(dsrc, k, n, seen, fa, lv);
     unsigned long long* front = fa;
     unsigned long long* next = fb;
+    unsigned long long live = full;  // sources whose frontier is not empty
     for (int32_t d = 0;; ++d) {
       // direction: push when the frontier's arcs are few (Beamer's rule against all arcs)
       GRE_CUDA(cudaMemsetAsync(cnt, 0, 64, g->stream));
       ms::k_frontier_list<<<grid_for(n, 256, 8), 256, 0, g->stream>>>(n, front, g->off, flist, (unsigned int*)(cnt + 2), cnt + 3);
-      unsigned long long h[5];
+      unsigned long long h[6];
       GRE_CUDA(cudaMemcpyAsync(h, cnt, sizeof(unsigned long long) * 4, cudaMemcpyDeviceToHost, g->stream));
       GRE_CUDA(cudaStreamSynchronize(g->stream));
       const bool push = h[3] * 14 < g->m;
@@ -485,12 +486,13 @@ int gre_msbfs(gre_graph g, const uint32_t* srcs, uint32_t nsrc, int32_t* levels,
         ms::k_push<<<grid_for((h[2] & 0xffffffffull) * 32, 256, 8), 256, 0, g->stream>>>(flist, (unsigned int*)(cnt + 2), g->off,
                                                                                           g->col, front, seen, acc);
       else
-        GRE_CHECK(ms::pull(g->bins_in, full, g->roff, g->rcol, front, seen, acc, cnt + 4, g->stream));
-      ms::k_commit<<<grid_for(n, 256, 8), 256, 0, g->stream>>>(n, acc, seen, next, lv, d + 1, cnt);
+        GRE_CHECK(ms::pull(g->bins_in, live, g->roff, g->rcol, front, seen, acc, cnt + 4, g->stream));
+      ms::k_commit<<<grid_for(n, 256, 8), 256, 0, g->stream>>>(n, acc, seen, next, lv, d + 1, cnt, cnt + 5);
       GRE_LAUNCH_CHECK();
       GRE_CUDA(cudaMemcpyAsync(h, cnt, sizeof h, cudaMemcpyDeviceToHost, g->stream));
       GRE_CUDA(cudaStreamSynchronize(g->stream));
       const unsigned long long found_bits = h[1];
+      live = h[5];
       if (push) {
         scanned += h[3];
         bytes += 16 * (h[2] & 0xffffffffull) + 12 * h[3] + 32 * n;

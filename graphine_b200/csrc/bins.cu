@@ -93,14 +93,6 @@ struct ProbeGather {
   const uint32_t* __restrict__ col;
   const double* __restrict__ x;
   __device__ __forceinline__ double operator()(uint32_t, uint64_t a) const { return __ldg(x + __ldg(col + a)); }
-  static constexpr bool kQuad = true;  // as GatherContrib: the tuner times the loads the superstep issues
-  __device__ __forceinline__ void quad(uint32_t, uint64_t a, double y[4]) const {
-    const uint4 c = __ldg((const uint4*)(col + a));
-    y[0] = __ldg(x + c.x);
-    y[1] = __ldg(x + c.y);
-    y[2] = __ldg(x + c.z);
-    y[3] = __ldg(x + c.w);
-  }
 };
 struct ProbeStore {
   double* __restrict__ y;

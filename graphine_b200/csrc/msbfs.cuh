@@ -144,12 +144,15 @@ static inline int pull(const DegreeBins& B, unsigned long long full, const uint6
 // fnext[v] = acc[v]; seen[v] |= acc[v]; acc[v] = 0.  When `levels` is given (k sources, rows of
 // n int32), writes next_level for every new (source, vertex) pair, one bit at a time across the
 // warp so that the writes of one source coalesce.  counters[0] += vertices with new bits,
-// counters[1] += new (source, vertex) pairs.
+// counters[1] += new (source, vertex) pairs, *live |= every new bit: the sources whose next
+// frontier is not empty.  Only those can reach a vertex at the next level, so the pull stops
+// looking for the others (a source in a small component would otherwise keep every vertex of
+// the large one scanning all its arcs at every level).
 static __global__ void k_commit(uint64_t n, unsigned long long* __restrict__ acc, unsigned long long* __restrict__ seen,
                                 unsigned long long* __restrict__ fnext, int32_t* __restrict__ levels, int32_t next_level,
-                                unsigned long long* __restrict__ counters) {
+                                unsigned long long* __restrict__ counters, unsigned long long* __restrict__ live) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  unsigned long long found_v = 0, found_bits = 0;
+  unsigned long long found_v = 0, found_bits = 0, any_bits = 0;
   for (uint64_t base = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) & ~31ull; base < n; base += stride) {
     const uint64_t v = base + (threadIdx.x & 31u);
     unsigned long long nb = 0;
@@ -173,6 +176,12 @@ static __global__ void k_commit(uint64_t n, unsigned long long* __restrict__ acc
     }
     found_v += nb != 0ull;
     found_bits += __popcll(nb);
+    any_bits |= nb;
+  }
+  {
+    const unsigned int lo = __reduce_or_sync(0xffffffffu, (unsigned int)(any_bits & 0xffffffffull));
+    const unsigned int hi = __reduce_or_sync(0xffffffffu, (unsigned int)(any_bits >> 32));
+    any_bits = ((unsigned long long)hi << 32) | lo;
   }
   for (int o = 16; o > 0; o >>= 1) {
     found_v += __shfl_xor_sync(0xffffffffu, found_v, o);
@@ -181,6 +190,7 @@ static __global__ void k_commit(uint64_t n, unsigned long long* __restrict__ acc
   if ((threadIdx.x & 31u) == 0) {
     if (found_v) atomicAdd(counters, found_v);
     if (found_bits) atomicAdd(counters + 1, found_bits);
+    if (any_bits && live) atomicOr(live, any_bits);
   }
 }
 

@@ -30,14 +30,6 @@ struct GatherContrib {
   const double* __restrict__ contrib;
   // contrib is read-only during a superstep (the next values go to the other buffer)
   __device__ __forceinline__ double operator()(uint32_t, uint64_t a) const { return __ldg(contrib + __ldg(rcol + a)); }
-  static constexpr bool kQuad = true;  // four columns per 16-byte load (a is a multiple of 4)
-  __device__ __forceinline__ void quad(uint32_t, uint64_t a, double x[4]) const {
-    const uint4 c = __ldg((const uint4*)(rcol + a));
-    x[0] = __ldg(contrib + c.x);
-    x[1] = __ldg(contrib + c.y);
-    x[2] = __ldg(contrib + c.z);
-    x[3] = __ldg(contrib + c.w);
-  }
 };
 
 struct FinishPR {

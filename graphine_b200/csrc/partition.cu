@@ -249,14 +249,6 @@ struct PartGather {
   const uint32_t* __restrict__ col;
   const double* __restrict__ contrib;  // all P * L slots
   __device__ __forceinline__ double operator()(uint32_t, uint64_t a) const { return __ldg(contrib + __ldg(col + a)); }
-  static constexpr bool kQuad = true;
-  __device__ __forceinline__ void quad(uint32_t, uint64_t a, double x[4]) const {
-    const uint4 c = __ldg((const uint4*)(col + a));
-    x[0] = __ldg(contrib + c.x);
-    x[1] = __ldg(contrib + c.y);
-    x[2] = __ldg(contrib + c.z);
-    x[3] = __ldg(contrib + c.w);
-  }
 };
 
 // pr = tele + d * sum; the power iteration refreshes the owner's contribution pr / outdeg

@@ -14,86 +14,12 @@
 //   Gather: __device__ double operator()(uint32_t row, uint64_t arc) const   value of one arc
 //   Finish: __device__ void operator()(uint32_t row, double sum) const
 #pragma once
-#include <cstdlib>
-#include <type_traits>
-
 #include "gre_internal.cuh"
 
 namespace gre {
 namespace rows {
 
 constexpr int kCta = 256;
-
-// Quad traversal (rows of 8 or more lanes per row, CTA rows and chunks): lane j adds the arcs
-// of quads j, j+L, j+2L, ... (a quad = four consecutive arcs starting at a multiple of 4), plus
-// one head and one tail arc where the row does not start or end on a quad.  A Gather that can
-// read a quad's four columns with one 16-byte load declares `static constexpr bool kQuad = true`
-// and quad(v, a, x[4]); the others are called four times.  Either way the association order is
-// that of the quads, the same for every Gather, so two paths over the same rows (the one-GPU
-// and the partitioned PageRank) still agree bit for bit.  The form halves the load instructions
-// per arc of the long rows, whose warps otherwise wait on the load/store queue (lg and mio
-// throttle stalls).  GRE_ROW_QUADS=0 selects the strided traversal instead.
-template <class Gather, class = void>
-struct has_quad : std::false_type {};
-template <class Gather>
-struct has_quad<Gather, std::void_t<decltype(Gather::kQuad)>> : std::bool_constant<Gather::kQuad> {};
-
-template <class Gather>
-__device__ __forceinline__ void quad(Gather& gat, uint32_t v, uint64_t a, double x[4]) {
-  if constexpr (has_quad<Gather>::value) {
-    gat.quad(v, a, x);
-  } else {
-    x[0] = gat(v, a);
-    x[1] = gat(v, a + 1);
-    x[2] = gat(v, a + 2);
-    x[3] = gat(v, a + 3);
-  }
-}
-
-inline bool quads_enabled() {
-  const char* e = getenv("GRE_ROW_QUADS");
-  return !e || strtoul(e, nullptr, 10) != 0;
-}
-
-// Sum of gat(v, a) over [a0, a1) in the quad traversal (L >= 4 lanes: the head and the tail have
-// at most three arcs each).  Two quads (eight gathers) in flight per lane.
-template <int L, class Gather>
-__device__ __forceinline__ double quad_sum(Gather& gat, uint32_t v, uint64_t a0, uint64_t a1, uint32_t lig) {
-  static_assert(L >= 4, "the head and tail need three lanes");
-  double acc = 0.0;
-  uint64_t q0 = (a0 + 3) & ~3ull;
-  if (q0 > a1) q0 = a1;
-  uint64_t q1 = a1 & ~3ull;
-  if (q1 < q0) q1 = q0;
-  if (a0 + lig < q0) acc += gat(v, a0 + lig);
-  uint64_t a = q0 + 4 * (uint64_t)lig;
-  for (; a + 4 * (uint64_t)L < q1; a += 8 * (uint64_t)L) {
-    double x[4], y[4];
-    quad(gat, v, a, x);
-    quad(gat, v, a + 4 * (uint64_t)L, y);
-    acc += x[0];
-    acc += x[1];
-    acc += x[2];
-    acc += x[3];
-    acc += y[0];
-    acc += y[1];
-    acc += y[2];
-    acc += y[3];
-  }
-  if (a < q1) {
-    double x[4];
-    quad(gat, v, a, x);
-    acc += x[0];
-    acc += x[1];
-    acc += x[2];
-    acc += x[3];
-  }
-  if (q1 + lig < a1) acc += gat(v, q1 + lig);
-  return acc;
-}
-
-template <int L, bool Q, class Gather>
-__device__ __forceinline__ double row_sum(Gather& gat, uint32_t v, uint64_t a0, uint64_t a1, uint32_t lig);
 
 // Sum of gat(v, a) over a = a0 + lig, a0 + lig + L, ... < a1.  Four arcs per pass so that each
 // lane has four independent (column, gathered value) load chains in flight: the loop is bound
@@ -113,13 +39,7 @@ __device__ __forceinline__ double strided_sum(Gather& gat, uint32_t v, uint64_t 
   return acc;
 }
 
-template <int L, bool Q, class Gather>
-__device__ __forceinline__ double row_sum(Gather& gat, uint32_t v, uint64_t a0, uint64_t a1, uint32_t lig) {
-  if constexpr (Q && L >= 8) return quad_sum<L>(gat, v, a0, a1, lig);
-  else return strided_sum<L>(gat, v, a0, a1, lig);
-}
-
-template <int L, bool Q, class Gather, class Finish>
+template <int L, class Gather, class Finish>
 __global__ void __launch_bounds__(256) k_rows_lanes(const uint32_t* __restrict__ rows, uint64_t count,
                                                      const uint64_t* __restrict__ off, Gather gat, Finish fin) {
   constexpr int G = 32 / L;  // groups per warp
@@ -135,7 +55,7 @@ __global__ void __launch_bounds__(256) k_rows_lanes(const uint32_t* __restrict__
     uint32_t v = 0;
     if (valid) {
       v = rows[i];
-      acc = row_sum<L, Q>(gat, v, off[v], off[v + 1], lig);
+      acc = strided_sum<L>(gat, v, off[v], off[v + 1], lig);
     }
 #pragma unroll
     for (int o = L / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -157,19 +77,19 @@ __device__ __forceinline__ double block_sum(double x, double* smem) {
   return t;  // valid in thread 0
 }
 
-template <bool Q, class Gather, class Finish>
+template <class Gather, class Finish>
 __global__ void __launch_bounds__(kCta) k_rows_cta(const uint32_t* __restrict__ rows, uint64_t count,
                                                     const uint64_t* __restrict__ off, Gather gat, Finish fin) {
   __shared__ double smem[kCta / 32];
   for (uint64_t i = blockIdx.x; i < count; i += gridDim.x) {
     const uint32_t v = rows[i];
-    double acc = row_sum<kCta, Q>(gat, v, off[v], off[v + 1], threadIdx.x);
+    double acc = strided_sum<kCta>(gat, v, off[v], off[v + 1], threadIdx.x);
     acc = block_sum(acc, smem);
     if (threadIdx.x == 0) fin(v, acc);
   }
 }
 
-template <bool Q, class Gather>
+template <class Gather>
 __global__ void __launch_bounds__(kCta) k_rows_chunks(const uint32_t* __restrict__ rows, const uint64_t* __restrict__ chunk_row,
                                                        const uint64_t* __restrict__ chunk_begin, uint64_t nchunks, uint64_t chunk,
                                                        const uint64_t* __restrict__ off, Gather gat, double* __restrict__ partial) {
@@ -179,21 +99,21 @@ __global__ void __launch_bounds__(kCta) k_rows_chunks(const uint32_t* __restrict
     const uint64_t a0 = chunk_begin[c];
     const uint64_t end = off[v + 1];
     const uint64_t a1 = (a0 + chunk < end) ? a0 + chunk : end;
-    double acc = row_sum<kCta, Q>(gat, v, a0, a1, threadIdx.x);
+    double acc = strided_sum<kCta>(gat, v, a0, a1, threadIdx.x);
     acc = block_sum(acc, smem);
     if (threadIdx.x == 0) partial[c] = acc;
   }
 }
 
 // Window-split rows (DegreeBins::seg_*): CTA per chunk in processing order, partial sums by slot.
-template <bool Q, class Gather>
+template <class Gather>
 __global__ void __launch_bounds__(kCta) k_rows_seg(const uint32_t* __restrict__ row, const uint64_t* __restrict__ begin,
                                                    const uint64_t* __restrict__ end, const uint64_t* __restrict__ slot,
                                                    uint64_t nchunks, Gather gat, double* __restrict__ partial) {
   __shared__ double smem[kCta / 32];
   for (uint64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
     const uint32_t v = row[c];
-    double acc = row_sum<kCta, Q>(gat, v, begin[c], end[c], threadIdx.x);
+    double acc = strided_sum<kCta>(gat, v, begin[c], end[c], threadIdx.x);
     acc = block_sum(acc, smem);
     if (threadIdx.x == 0) partial[slot[c]] = acc;
   }
@@ -220,36 +140,31 @@ __global__ void k_rows_chunk_finish(const uint32_t* __restrict__ rows, uint64_t 
 }
 
 // Launch the reductions of every non-empty row.  `partial` holds bins.n_hub_chunks doubles.
-template <bool Q, class Gather, class Finish>
-int reduce_rows_t(const DegreeBins& B, const uint64_t* off, Gather gat, Finish fin, double* partial, cudaStream_t s) {
+template <class Gather, class Finish>
+int reduce_rows(const DegreeBins& B, const uint64_t* off, Gather gat, Finish fin, double* partial, cudaStream_t s) {
   const uint32_t* r = B.rows;
   auto grid = [](uint64_t threads) { return grid_for(threads, 256, 8); };
-  if (B.count[0]) k_rows_lanes<1, Q><<<grid(B.count[0]), 256, 0, s>>>(r + B.start[0], B.count[0], off, gat, fin);
-  if (B.count[1]) k_rows_lanes<2, Q><<<grid(B.count[1] * 2), 256, 0, s>>>(r + B.start[1], B.count[1], off, gat, fin);
-  if (B.count[2]) k_rows_lanes<4, Q><<<grid(B.count[2] * 4), 256, 0, s>>>(r + B.start[2], B.count[2], off, gat, fin);
-  if (B.count[3]) k_rows_lanes<8, Q><<<grid(B.count[3] * 8), 256, 0, s>>>(r + B.start[3], B.count[3], off, gat, fin);
-  if (B.count[4]) k_rows_lanes<16, Q><<<grid(B.count[4] * 16), 256, 0, s>>>(r + B.start[4], B.count[4], off, gat, fin);
-  if (B.count[5]) k_rows_lanes<32, Q><<<grid(B.count[5] * 32), 256, 0, s>>>(r + B.start[5], B.count[5], off, gat, fin);
+  if (B.count[0]) k_rows_lanes<1><<<grid(B.count[0]), 256, 0, s>>>(r + B.start[0], B.count[0], off, gat, fin);
+  if (B.count[1]) k_rows_lanes<2><<<grid(B.count[1] * 2), 256, 0, s>>>(r + B.start[1], B.count[1], off, gat, fin);
+  if (B.count[2]) k_rows_lanes<4><<<grid(B.count[2] * 4), 256, 0, s>>>(r + B.start[2], B.count[2], off, gat, fin);
+  if (B.count[3]) k_rows_lanes<8><<<grid(B.count[3] * 8), 256, 0, s>>>(r + B.start[3], B.count[3], off, gat, fin);
+  if (B.count[4]) k_rows_lanes<16><<<grid(B.count[4] * 16), 256, 0, s>>>(r + B.start[4], B.count[4], off, gat, fin);
+  if (B.count[5]) k_rows_lanes<32><<<grid(B.count[5] * 32), 256, 0, s>>>(r + B.start[5], B.count[5], off, gat, fin);
   if (B.seg_nchunks) {  // rows above cta_min, window by window
-    k_rows_seg<Q><<<grid_for(B.seg_nchunks * kCta, kCta, 8), kCta, 0, s>>>(B.seg_row, B.seg_begin, B.seg_end, B.seg_slot,
-                                                                            B.seg_nchunks, gat, partial);
+    k_rows_seg<<<grid_for(B.seg_nchunks * kCta, kCta, 8), kCta, 0, s>>>(B.seg_row, B.seg_begin, B.seg_end, B.seg_slot,
+                                                                         B.seg_nchunks, gat, partial);
     k_rows_seg_finish<<<grid_for(B.seg_nrows, 128, 4), 128, 0, s>>>(B.seg_rows, B.seg_nrows, B.seg_first, partial, fin);
     GRE_LAUNCH_CHECK();
     return GRE_SUCCESS;
   }
-  if (B.count[6]) k_rows_cta<Q><<<grid_for(B.count[6] * kCta, kCta, 8), kCta, 0, s>>>(r + B.start[6], B.count[6], off, gat, fin);
+  if (B.count[6]) k_rows_cta<<<grid_for(B.count[6] * kCta, kCta, 8), kCta, 0, s>>>(r + B.start[6], B.count[6], off, gat, fin);
   if (B.count[7]) {
-    k_rows_chunks<Q><<<grid_for(B.n_hub_chunks * kCta, kCta, 8), kCta, 0, s>>>(r + B.start[7], B.hub_chunk_row, B.hub_chunk_begin,
-                                                                               B.n_hub_chunks, B.sched.hub_chunk, off, gat, partial);
+    k_rows_chunks<<<grid_for(B.n_hub_chunks * kCta, kCta, 8), kCta, 0, s>>>(r + B.start[7], B.hub_chunk_row, B.hub_chunk_begin,
+                                                                            B.n_hub_chunks, B.sched.hub_chunk, off, gat, partial);
     k_rows_chunk_finish<<<grid_for(B.count[7], 128, 4), 128, 0, s>>>(r + B.start[7], B.count[7], B.hub_chunk_first, partial, fin);
   }
   GRE_LAUNCH_CHECK();
   return GRE_SUCCESS;
-}
-
-template <class Gather, class Finish>
-int reduce_rows(const DegreeBins& B, const uint64_t* off, Gather gat, Finish fin, double* partial, cudaStream_t s) {
-  return quads_enabled() ? reduce_rows_t<true>(B, off, gat, fin, partial, s) : reduce_rows_t<false>(B, off, gat, fin, partial, s);
 }
 
 // Number of non-empty rows of the bins (for byte models).

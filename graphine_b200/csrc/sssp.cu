@@ -707,9 +707,9 @@ static uint64_t binned_frontier() {
   return 64;
 }
 
-// Whether those large passes pull (over the vertices that can still improve) instead of pushing
-// (along the frontier's arcs), where the weights allow it (g->w32_symmetric).  Default on; the
-// GRE_SSSP_PULL environment variable set to 0 keeps the push form.
+// Whether the large heavy passes pull (over the vertices that can still improve) instead of
+// pushing (along the bucket's heavy arcs), where the weights allow it (g->w32_symmetric).
+// Default on; the GRE_SSSP_PULL environment variable set to 0 keeps the push form.
 static bool pull_enabled() {
   if (const char* e = getenv("GRE_SSSP_PULL")) return strtoul(e, nullptr, 10) != 0;
   return true;
@@ -840,11 +840,11 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
         k_queue_to_bits<<<grid_for(nlist, 256), 256, 0, g->stream>>>(list, nlist, front);
       }
       GRE_CHECK(init_counters(g, cnt, 0, (uint32_t)nfar, (uint32_t)nb));
-      if (pull) {
-        // light pass: every vertex outside the settled buckets may improve; heavy pass: only
-        // vertices at or above the limit (heavy arcs from the bucket land there)
-        const uint32_t lo = heavy ? limit : (limit > delta ? limit - delta : 0u);
-        PullRange P{front, off, lend, col, w, dist, changed, pull_counts, heavy, lo};
+      if (pull && heavy) {
+        // the bucket's heavy arcs: only vertices at or above the limit can improve (heavy arcs
+        // from the bucket land there).  (Light passes push: every unsettled vertex would have to
+        // scan its light arcs at every pass of the bucket, measured slower than the push.)
+        PullRange P{front, off, lend, col, w, dist, changed, pull_counts, true, limit};
         GRE_CHECK(pull_binned(bins, P, g->stream));
         bytes += 16 * n;  // per row: its id, distance and range bounds (arcs at the end)
       } else {

@@ -136,7 +136,7 @@ def test_bc_on_a_long_path(batched):
 
     The fast paths run BFS/BC to completion.  The reference engine stops every run after its
     default 1024 supersteps (Engine.hpp:108, which usr/test_bc.cpp does not raise), so on this
-    graph its levels end at 1023; the device engine (gre_vc_*) keeps that limit, and the oracle
+    graph its levels end at 1024; the device engine (gre_vc_*) keeps that limit, and the oracle
     restates it, which is why the closed form is the reference here."""
     n = 6000
     edges = [(i, i + 1) for i in range(n - 1)] + [(i + 1, i) for i in range(n - 1)]
@@ -152,4 +152,4 @@ def test_bc_on_a_long_path(batched):
     lv, _ = G.bfs(g, roots[:1])
     np.testing.assert_array_equal(lv, np.arange(n))
     R = O.Restatement.from_csr(n, off, col)  # the reference's engine limit, restated
-    assert R.bfs(0)[0].max() == 1023
+    assert R.bfs(0)[0].max() == 1024
