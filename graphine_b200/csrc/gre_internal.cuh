@@ -350,11 +350,25 @@ int sssp_delta(gre_graph g, uint32_t* delta);
 // ceil(total / sssp_tile_arcs()) entries; error is set if a tile holds too many owners.
 uint64_t sssp_tile_arcs();
 // The binned form of a relaxation pass as offers (sssp.cu): every row of the bins whose bit is set
-// in `front` offers srcdist[row] + w over all its arcs [off[row], off[row+1]) into `offers`
-// (atomic min); `arcs` counts the arcs.
+// in `front` offers srcdist[row] + w over its light arcs [off[row], lend[row]) (heavy: [lend[row],
+// off[row+1])) into `offers` (atomic min); `arcs` (may be null) counts the arcs.
 int sssp_relax_binned_offer(cudaStream_t stream, const DegreeBins& B, const uint32_t* front, const uint64_t* off,
-                            const uint32_t* col, const uint32_t* w, const uint32_t* srcdist, uint32_t* offers,
-                            unsigned long long* arcs);
+                            const uint64_t* lend, bool heavy, const uint32_t* col, const uint32_t* w, const uint32_t* srcdist,
+                            uint32_t* offers, unsigned long long* arcs);
+// The pull form of a pass (sssp.cu; symmetric graph with symmetric weights): every row whose
+// dist[row] >= lo takes the smallest srcdist[u] + w over its light (heavy) arcs to columns u set
+// in `front`; an improvement lowers dist[row] and sets the row's bit in `changed`.  counts[0] +=
+// arcs scanned, counts[1] += frontier hits.
+int sssp_pull_binned(cudaStream_t stream, const DegreeBins& B, const uint32_t* front, const uint64_t* off, const uint64_t* lend,
+                     bool heavy, const uint32_t* col, const uint32_t* w, const uint32_t* srcdist, uint32_t* dist, uint32_t* changed,
+                     uint32_t lo, unsigned long long* counts);
+// Light/heavy split of `rows` rows for bucket width delta (sssp.cu): light arcs (w < delta) first.
+int sssp_split_rows(cudaStream_t stream, uint64_t rows, const uint64_t* off, const uint32_t* col, const uint32_t* w, uint32_t delta,
+                    uint32_t* ocol, uint32_t* ow, uint64_t* lend);
+// Frontiers of at least n / sssp_binned_divisor() vertices go through the degree bins (0: never);
+// whether heavy passes may pull (GRE_SSSP_BINNED, GRE_SSSP_PULL).
+uint64_t sssp_binned_divisor();
+bool sssp_pull_enabled();
 int sssp_relax_tiles(cudaStream_t stream, const uint32_t* queue, uint64_t nq, const uint64_t* prefix, uint64_t total,
                      uint32_t* tstart, const uint64_t* base, const uint32_t* col, const uint32_t* w, const uint32_t* srcdist,
                      uint32_t* dist, uint32_t* changed, uint32_t* error);

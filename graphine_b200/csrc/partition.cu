@@ -54,6 +54,11 @@ struct gre_part_s {
   uint32_t* xof = nullptr;   // caller id -> exchange index (n)
   uint32_t* xmap = nullptr;  // exchange index -> caller id, 0xffffffff for padding (P * L)
   uint64_t cc_remote = ~0ull;  // arcs of the owned rows that lead to another rank (counted on first use)
+  bool w_sym = false;          // the graph's weights are symmetric (w32_symmetric): SSSP may pull
+  // SSSP light/heavy split of the owned out-rows for `delta` (built on first use): light arcs first
+  uint32_t* sp_col = nullptr;
+  uint32_t* sp_w = nullptr;
+  uint64_t* sp_lend = nullptr;
 };
 
 namespace gre {
@@ -313,25 +318,31 @@ __global__ void k_part_sssp_claim(uint64_t L, uint64_t P, const uint32_t* __rest
   }
 }
 
-// Near-far selection (Davidson et al., IPDPS 2014): pending slots below the limit form this
-// superstep's frontier (their pending bits are cleared); the others stay pending, and the
-// smallest of their distances is kept (to raise the limit when the near set runs dry).
+// Near-far selection with the light/heavy split of delta-stepping (Davidson et al., IPDPS 2014;
+// Meyer and Sanders 2003), as the one-GPU path: pending slots below the limit leave the pending
+// set; those with light arcs ([off, lend)) form this superstep's light frontier, those with heavy
+// arcs ([lend, off+1)) join the bucket, whose heavy arcs are relaxed once when no rank has a
+// light frontier left.  The other pending slots stay, and the smallest of their distances is
+// kept (to raise the limit when the bucket is done).  One lane owns each pending word.
 struct SsspCounters {
-  unsigned long long near;     // queued this superstep
-  unsigned long long pending;  // left pending (at or above the limit)
-  unsigned long long min_far;  // smallest distance left pending
-  unsigned long long arcs;     // out-arcs of the queued slots
+  unsigned long long near;        // light frontier of this superstep
+  unsigned long long pending;     // left pending (at or above the limit)
+  unsigned long long min_far;     // smallest distance left pending
+  unsigned long long arcs;        // light arcs of the frontier
+  unsigned long long bucket_new;  // slots that joined the bucket
+  unsigned long long pad[3];
 };
 
 __global__ void k_part_sssp_select(uint64_t W, uint32_t* __restrict__ pend, const uint32_t* __restrict__ dist, uint32_t limit,
-                                   const uint32_t* __restrict__ outdeg, uint32_t* __restrict__ queue,
-                                   SsspCounters* __restrict__ c) {
+                                   const uint64_t* __restrict__ off, const uint64_t* __restrict__ lend, uint32_t* __restrict__ inb,
+                                   uint32_t* __restrict__ queue, SsspCounters* __restrict__ c) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  unsigned long long left = 0, arcs = 0;
+  unsigned long long left = 0, arcs = 0, joined = 0;
   uint32_t dmin = 0xffffffffu;
   for (uint64_t base = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) & ~31ull; base < W; base += stride) {
     const uint64_t w = base + (threadIdx.x & 31u);
-    uint32_t bits = w < W ? pend[w] : 0u, keep = 0;
+    uint32_t bits = w < W ? pend[w] : 0u, keep = 0, join = 0;
+    const uint32_t inw = bits ? inb[w] : 0u;
     while (__any_sync(0xffffffffu, bits != 0)) {
       bool take = false;
       uint32_t i = 0;
@@ -341,8 +352,10 @@ __global__ void k_part_sssp_select(uint64_t W, uint32_t* __restrict__ pend, cons
         i = (uint32_t)(w << 5) + b;
         const uint32_t d = dist[i];
         if (d < limit) {
-          take = outdeg[i] != 0;  // a source without out-arcs has nothing to offer
-          arcs += outdeg[i];
+          const uint64_t a0 = off[i], am = lend[i], a1 = off[i + 1];
+          take = am > a0;
+          arcs += am - a0;
+          if (a1 > am && !((inw >> b) & 1u)) join |= 1u << b;
         } else {
           keep |= 1u << b;
           ++left;
@@ -353,16 +366,31 @@ __global__ void k_part_sssp_select(uint64_t W, uint32_t* __restrict__ pend, cons
       if (take) queue[pos] = i;
     }
     if (w < W && pend[w] != keep) pend[w] = keep;
+    if (join) {
+      inb[w] = inw | join;
+      joined += __popc(join);
+    }
   }
   dmin = __reduce_min_sync(0xffffffffu, dmin);
   for (int o = 16; o > 0; o >>= 1) {
     left += __shfl_xor_sync(0xffffffffu, left, o);
     arcs += __shfl_xor_sync(0xffffffffu, arcs, o);
+    joined += __shfl_xor_sync(0xffffffffu, joined, o);
   }
   if ((threadIdx.x & 31u) == 0) {
     if (left) atomicAdd(&c->pending, left);
     if (arcs) atomicAdd(&c->arcs, arcs);
+    if (joined) atomicAdd(&c->bucket_new, joined);
     if (dmin != 0xffffffffu) atomicMin(&c->min_far, (unsigned long long)dmin);
+  }
+}
+
+// arcs of the queued slots in their light ([off, lend)) or heavy ([lend, off+1)) range
+__global__ void k_part_range_degrees(const uint32_t* __restrict__ queue, uint64_t nq, const uint64_t* __restrict__ off,
+                                     const uint64_t* __restrict__ lend, bool heavy, uint64_t* __restrict__ deg) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nq; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t v = queue[i];
+    deg[i] = heavy ? off[v + 1] - lend[v] : lend[v] - off[v];
   }
 }
 
@@ -560,6 +588,9 @@ void destroy_part(gre_part p) {
     cudaFree(p->xof);
     cudaFree(p->xmap);
     cudaFree(p->w32);
+    cudaFree(p->sp_col);
+    cudaFree(p->sp_w);
+    cudaFree(p->sp_lend);
     destroy_graph(p->sub);
   }
   delete p;
@@ -620,6 +651,7 @@ int gre_part_create(gre_graph g, uint32_t nparts, uint32_t rank, gre_part* out) 
       k_part_weights<<<grid_for(L * 32, 256, 8), 256, 0, s->stream>>>(L, rank, P, n, g->off, g->w32, s->off, p->w32);
       GRE_LAUNCH_CHECK();
       GRE_CHECK(sssp_delta(g, &p->delta));  // the whole graph's, the same on every rank
+      p->w_sym = g->w32_symmetric && g->symmetric();
     }
     GRE_CUDA(cudaMalloc(&p->xof, sizeof(uint32_t) * (n ? n : 1)));
     GRE_CUDA(cudaMalloc(&p->xmap, sizeof(uint32_t) * P * L));
@@ -854,7 +886,20 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
     set_error("gre_part_sssp: source %u out of range (n = %llu)", src, (unsigned long long)n);
     return GRE_INVALID_ARG;
   }
-  uint32_t *dl, *dist_all, *queue, *pend, *cand, *recv, *dout;
+  // the light/heavy split of the owned out-rows (once per part; delta is the whole graph's)
+  const uint32_t delta = p->delta;
+  if (delta && !p->sp_lend) {
+    GRE_CUDA(cudaMalloc(&p->sp_col, sizeof(uint32_t) * (p->arcs_out ? p->arcs_out : 1)));
+    GRE_CUDA(cudaMalloc(&p->sp_w, sizeof(uint32_t) * (p->arcs_out ? p->arcs_out : 1)));
+    GRE_CUDA(cudaMalloc(&p->sp_lend, sizeof(uint64_t) * L));
+    GRE_CHECK(sssp_split_rows(s->stream, L, s->off, s->col, p->w32, delta, p->sp_col, p->sp_w, p->sp_lend));
+  }
+  const uint64_t* off = s->off;
+  const uint64_t* lend = delta ? p->sp_lend : s->off + 1;  // end of each row's light arcs
+  const uint32_t* col = delta ? p->sp_col : s->col;
+  const uint32_t* w = delta ? p->sp_w : p->w32;
+  const DegreeBins& B = s->roff == s->off ? s->bins_in : s->bins_out;
+  uint32_t *dl, *dist_all, *queue, *pend, *inb, *inb_all, *cand, *recv, *dout;
   uint64_t *deg, *prefix;
   SsspCounters *c, *call;
   BfsCounters *bc, *bcall;
@@ -862,30 +907,36 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
   GRE_CHECK(ws_array(s, WS_B, P * L, &dist_all));
   GRE_CHECK(ws_array(s, WS_C, W, &pend));
   GRE_CHECK(ws_array(s, WS_D, L, &queue));
+  GRE_CHECK(ws_array(s, WS_F, W, &inb));
+  GRE_CHECK(ws_array(s, WS_G, P * W, &inb_all));
   GRE_CHECK(ws_array(s, WS_I, P * L, &cand));
   GRE_CHECK(ws_array(s, WS_J, P * L, &recv));
   GRE_CHECK(ws_array(s, WS_K, L + 1, &deg));
   GRE_CHECK(ws_array(s, WS_L, L + 1, &prefix));
   uint32_t *tstart, *err;
   GRE_CHECK(ws_array(s, WS_E, p->arcs_out / sssp_tile_arcs() + 2, &tstart));
-  GRE_CHECK(ws_array(s, WS_COUNTERS, 3, &c));
+  GRE_CHECK(ws_array(s, WS_COUNTERS, 4, &c));  // c[0] counters, c[1] BFS-style totals, c[2] flags, c[3] pull counts
   GRE_CHECK(ws_array(s, WS_OUTBUF2, P, &call));
   bc = (BfsCounters*)(c + 1);
   err = (uint32_t*)(c + 2);
-  unsigned long long* arcs_seen = (unsigned long long*)(c + 2) + 1;  // arcs of binned passes (unused: the select counts them)
+  unsigned long long* pull_counts = (unsigned long long*)(c + 3);  // arcs scanned, hits
   bcall = (BfsCounters*)call;
   GRE_CHECK(prepare_output(s, dist, n, WS_OUTBUF, &dout));
   void* cubtmp = nullptr;
   size_t cubbytes = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, cubbytes, deg, prefix, L + 1, s->stream);
   GRE_CHECK(s->ws.get(WS_CUB, cubbytes, &cubtmp));
+  const uint64_t bdiv = sssp_binned_divisor();
+  const bool pull = p->w_sym && delta && sssp_pull_enabled();
 
   RunTimer timer(s);
   uint32_t xr = 0;
   GRE_CUDA(cudaMemcpyAsync(&xr, p->xof + src, sizeof xr, cudaMemcpyDeviceToHost, s->stream));
   GRE_CUDA(cudaMemsetAsync(dl, 0xff, sizeof(uint32_t) * L, s->stream));
   GRE_CUDA(cudaMemsetAsync(pend, 0, sizeof(uint32_t) * W, s->stream));
+  GRE_CUDA(cudaMemsetAsync(inb, 0, sizeof(uint32_t) * W, s->stream));
   GRE_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), s->stream));
+  GRE_CUDA(cudaMemsetAsync(pull_counts, 0, 2 * sizeof(unsigned long long), s->stream));
   GRE_CUDA(cudaStreamSynchronize(s->stream));
   if (xr / L == me) {
     const uint32_t slot = xr - (uint32_t)(me * L), zero = 0, bit = 1u << (slot & 31u);
@@ -893,17 +944,48 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
     GRE_CUDA(cudaMemcpyAsync(pend + (slot >> 5), &bit, sizeof bit, cudaMemcpyHostToDevice, s->stream));
   }
   // Supersteps of the reference's SSSP (every improved vertex scatters dist + w, combine = min),
-  // ordered near-far: only pending slots below a global limit scatter; when none is left
-  // anywhere, the limit moves to the smallest pending distance + delta (half the mean weight).
-  const uint32_t delta = p->delta ? p->delta : 0xffffffffu;
-  uint32_t limit = delta;
-  uint64_t relaxed = 0, bytes = 0;
+  // ordered as the one-GPU path: pending slots below a global limit relax their light arcs (offers
+  // to the owners: an all-to-all); when no rank has any left, the bucket's heavy arcs are relaxed
+  // once (pulled by the slots at or above the limit from all-gathered distances and bucket bits
+  // where the weights are symmetric, else offered); then the limit moves to the smallest pending
+  // distance + delta.
+  const uint32_t width = delta ? delta : 0xffffffffu;
+  uint32_t limit = width;
+  uint64_t relaxed = 0, bytes = 0, bucket = 0;
   uint32_t steps = 0;
   std::vector<SsspCounters> h(P);
+  // offers of this rank's frontier `list` (or bitmap `front`, binned form) over the light or heavy
+  // ranges, exchanged with the owners, who keep the smallest and mark improved slots pending
+  auto offer_pass = [&](const uint32_t* list, uint64_t nlist, const uint32_t* front, uint64_t arcs, bool heavy) -> int {
+    GRE_CUDA(cudaMemsetAsync(cand, 0xff, sizeof(uint32_t) * P * L, s->stream));
+    if (nlist && arcs && bdiv && nlist >= L / bdiv) {
+      uint32_t* bits = const_cast<uint32_t*>(front);
+      if (!bits) {  // the frontier as a bitmap, in the scan buffer (unused by this form)
+        bits = (uint32_t*)deg;
+        GRE_CUDA(cudaMemsetAsync(bits, 0, sizeof(uint32_t) * W, s->stream));
+        k_queue_to_bits<<<grid_for(nlist, 256), 256, 0, s->stream>>>(list, nlist, bits);
+        bytes += 4 * W + 4 * nlist;
+      }
+      GRE_CHECK(sssp_relax_binned_offer(s->stream, B, bits, off, lend, heavy, col, w, dl, cand, nullptr));
+      bytes += 16 * L + W * 4;  // rows scanned and their frontier bits (arcs below)
+    } else if (nlist && arcs) {
+      k_part_range_degrees<<<grid_for(nlist, 256), 256, 0, s->stream>>>(list, nlist, off, lend, heavy, deg);
+      GRE_CUDA(cub::DeviceScan::ExclusiveSum(cubtmp, cubbytes, deg, prefix, nlist + 1, s->stream));
+      GRE_CHECK(sssp_relax_tiles(s->stream, list, nlist, prefix, arcs, tstart, heavy ? lend : off, col, w, dl, cand, nullptr,
+                                 err));
+      bytes += 16 * nlist;
+    }
+    GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLTOALL, cand, recv, 4 * L));
+    k_part_sssp_claim<<<grid_for(L, 256), 256, 0, s->stream>>>(L, P, recv, dl, s->outdeg, pend);
+    GRE_LAUNCH_CHECK();
+    relaxed += arcs;
+    bytes += 12 * arcs + 4 * P * L * 3 + 4 * L;
+    return GRE_SUCCESS;
+  };
   for (;;) {
-    const SsspCounters zero{0, 0, 0xffffffffffffffffull, 0};
+    const SsspCounters zero{0, 0, 0xffffffffffffffffull, 0, 0, {0, 0, 0}};
     GRE_CUDA(cudaMemcpyAsync(c, &zero, sizeof zero, cudaMemcpyHostToDevice, s->stream));
-    k_part_sssp_select<<<grid_for(W, 256), 256, 0, s->stream>>>(W, pend, dl, limit, s->outdeg, queue, c);
+    k_part_sssp_select<<<grid_for(W, 256), 256, 0, s->stream>>>(W, pend, dl, limit, off, lend, inb, queue, c);
     GRE_LAUNCH_CHECK();
     GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLGATHER, c, call, sizeof(SsspCounters)));
     GRE_CUDA(cudaMemcpyAsync(h.data(), call, sizeof(SsspCounters) * P, cudaMemcpyDeviceToHost, s->stream));
@@ -912,39 +994,51 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
     for (const SsspCounters& x : h) {
       near += x.near;
       pending += x.pending;
+      bucket += x.bucket_new;
       min_far = std::min<uint64_t>(min_far, x.min_far);
     }
     bytes += 4 * W + 8 * (h[me].near + h[me].pending);
-    if (near == 0) {
-      if (pending == 0) break;
-      // every rank sees the same sums: the same new limit
-      limit = min_far > 0xffffffffull - delta ? 0xffffffffu : (uint32_t)(min_far + delta);
+    if (near) {  // a light superstep
+      GRE_CHECK(offer_pass(queue, h[me].near, nullptr, h[me].arcs, false));
+      ++steps;
+      stats_record(st, near);
       continue;
     }
-    const uint64_t nq = h[me].near;
-    GRE_CUDA(cudaMemsetAsync(cand, 0xff, sizeof(uint32_t) * P * L, s->stream));
-    unsigned long long total = h[me].arcs;
-    if (nq && total && nq >= L / 64) {
-      // a large frontier: the one-GPU path's binned relaxation over this rank's degree bins,
-      // the queued slots as a bitmap (in the scan buffer, unused by this form)
-      uint32_t* front = (uint32_t*)deg;
-      GRE_CUDA(cudaMemsetAsync(front, 0, sizeof(uint32_t) * W, s->stream));
-      k_queue_to_bits<<<grid_for(nq, 256), 256, 0, s->stream>>>(queue, nq, front);
-      GRE_LAUNCH_CHECK();
-      const DegreeBins& B = s->roff == s->off ? s->bins_in : s->bins_out;
-      GRE_CHECK(sssp_relax_binned_offer(s->stream, B, front, s->off, s->col, p->w32, dl, cand, arcs_seen));
-    } else if (nq && total) {  // the one-GPU path's tile relaxation: offers go to cand, owners' distances from dl
-      k_frontier_degrees<<<grid_for(nq, 256), 256, 0, s->stream>>>(queue, nq, s->off, deg);
-      GRE_CUDA(cub::DeviceScan::ExclusiveSum(cubtmp, cubbytes, deg, prefix, nq + 1, s->stream));
-      GRE_CHECK(sssp_relax_tiles(s->stream, queue, nq, prefix, total, tstart, s->off, s->col, p->w32, dl, cand, nullptr, err));
+    if (bucket) {  // the bucket is settled: its heavy arcs, once (every rank sees the same sums)
+      if (pull && bdiv && bucket >= P * L / bdiv) {
+        GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLGATHER, dl, dist_all, 4 * L));
+        GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLGATHER, inb, inb_all, 4 * W));
+        GRE_CHECK(sssp_pull_binned(s->stream, B, inb_all, off, lend, true, col, w, dist_all, dl, pend, limit, pull_counts));
+        bytes += 4 * P * L + 4 * P * W + 16 * L;
+      } else {
+        uint64_t nb = 0, arcs = 0;
+        {  // this rank's members as a queue (for the tiles) and the count of their heavy arcs
+          unsigned long long* cnt = (unsigned long long*)&bc->next_count;
+          GRE_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), s->stream));
+          k_bits_to_queue<<<grid_for(W, 256), 256, 0, s->stream>>>(L, inb, queue, cnt);
+          GRE_LAUNCH_CHECK();
+          unsigned long long hn = 0;
+          GRE_CUDA(cudaMemcpyAsync(&hn, cnt, sizeof hn, cudaMemcpyDeviceToHost, s->stream));
+          GRE_CUDA(cudaStreamSynchronize(s->stream));
+          nb = hn;
+          if (nb) {
+            k_part_range_degrees<<<grid_for(nb, 256), 256, 0, s->stream>>>(queue, nb, off, lend, true, deg);
+            GRE_CUDA(cub::DeviceScan::ExclusiveSum(cubtmp, cubbytes, deg, prefix, nb + 1, s->stream));
+            GRE_CUDA(cudaMemcpyAsync(&arcs, prefix + nb, sizeof arcs, cudaMemcpyDeviceToHost, s->stream));
+            GRE_CUDA(cudaStreamSynchronize(s->stream));
+          }
+        }
+        GRE_CHECK(offer_pass(queue, nb, inb, arcs, true));
+      }
+      GRE_CUDA(cudaMemsetAsync(inb, 0, sizeof(uint32_t) * W, s->stream));
+      bucket = 0;
+      ++steps;
+      stats_record(st, 0);
+      continue;
     }
-    GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLTOALL, cand, recv, 4 * L));
-    k_part_sssp_claim<<<grid_for(L, 256), 256, 0, s->stream>>>(L, P, recv, dl, s->outdeg, pend);
-    GRE_LAUNCH_CHECK();
-    relaxed += total;
-    bytes += 16 * nq + 12 * total + 4 * P * L * 3 + 4 * L;
-    ++steps;
-    stats_record(st, near);
+    if (pending == 0) break;
+    // every rank sees the same sums: the same new limit
+    limit = min_far > 0xffffffffull - width ? 0xffffffffu : (uint32_t)(min_far + width);
   }
   GRE_CUDA(cudaMemsetAsync(bc, 0, sizeof(BfsCounters), s->stream));
   k_part_reached_dist<<<grid_for(L, 256), 256, 0, s->stream>>>(L, dl, s->outdeg, &bc->next_arcs);
@@ -956,7 +1050,9 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
   GRE_LAUNCH_CHECK();
   // checked after the last collective, so that every rank takes the same ones
   uint32_t herr = 0;
+  unsigned long long pc[2] = {0, 0};
   GRE_CUDA(cudaMemcpyAsync(&herr, err, sizeof herr, cudaMemcpyDeviceToHost, s->stream));
+  GRE_CUDA(cudaMemcpyAsync(pc, pull_counts, sizeof pc, cudaMemcpyDeviceToHost, s->stream));
   GRE_CUDA(cudaStreamSynchronize(s->stream));
   if (herr) {
     set_error("gre_part_sssp: frontier tile overflow");
@@ -966,9 +1062,9 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
   GRE_CHECK(timer.stop(st));
   if (st) {
     st->supersteps = steps;
-    st->arcs_traversed = relaxed;  // this rank's
+    st->arcs_traversed = relaxed + pc[0];  // this rank's
     st->traversed_edges = s->symmetric() ? sum.next_arcs / 2 : sum.next_arcs;
-    st->algo_bytes = bytes;
+    st->algo_bytes = bytes + 4 * pc[0] + 8 * pc[1];
   }
   return GRE_SUCCESS;
 }

@@ -256,9 +256,10 @@ struct RelaxRange {
   }
 };
 
+// c may be null (the caller counts the arcs another way)
 __device__ __forceinline__ void add_arcs(unsigned long long* c, unsigned long long k) {
   for (int o = 16; o > 0; o >>= 1) k += __shfl_xor_sync(0xffffffffu, k, o);
-  if ((threadIdx.x & 31u) == 0 && k) atomicAdd(c, k);
+  if ((threadIdx.x & 31u) == 0 && k && c) atomicAdd(c, k);
 }
 
 template <int G, bool OFFER>
@@ -350,11 +351,13 @@ struct PullRange {
   const uint64_t* __restrict__ lend;
   const uint32_t* __restrict__ col;
   const uint32_t* __restrict__ w;
-  uint32_t* __restrict__ dist;
-  uint32_t* __restrict__ changed;
+  uint32_t* __restrict__ dist;               // the rows' distances (improved in place)
+  uint32_t* __restrict__ changed;            // a bit per improved row
   unsigned long long* __restrict__ counts;  // [0] arcs scanned, [1] frontier hits
   bool heavy;
   uint32_t lo;
+  const uint32_t* __restrict__ srcdist;      // the frontier's distances, indexed by column (the
+                                             // one-GPU path: dist itself)
   __device__ __forceinline__ void range(uint32_t v, uint64_t* a0, uint64_t* a1) const {
     *a0 = heavy ? lend[v] : off[v];
     *a1 = heavy ? off[v + 1] : lend[v];
@@ -373,7 +376,7 @@ struct PullRange {
 #pragma unroll
       for (int k = 0; k < 4; ++k)
         if (in[k]) {
-          const uint32_t nd = __ldcg(dist + u[k]) + __ldg(w + a + k * step);
+          const uint32_t nd = __ldcg(srcdist + u[k]) + __ldg(w + a + k * step);
           b = nd < b ? nd : b;
           ++*hits;
         }
@@ -381,7 +384,7 @@ struct PullRange {
     for (; a < hi; a += step) {
       const uint32_t u = __ldg(col + a);
       if ((__ldg(front + (u >> 5)) >> (u & 31u)) & 1u) {
-        const uint32_t nd = __ldcg(dist + u) + __ldg(w + a);
+        const uint32_t nd = __ldcg(srcdist + u) + __ldg(w + a);
         b = nd < b ? nd : b;
         ++*hits;
       }
@@ -523,10 +526,24 @@ __global__ void k_sssp_classes(uint64_t n, const uint64_t* __restrict__ off, con
 }
 
 int sssp_relax_binned_offer(cudaStream_t stream, const DegreeBins& B, const uint32_t* front, const uint64_t* off,
-                            const uint32_t* col, const uint32_t* w, const uint32_t* srcdist, uint32_t* offers,
-                            unsigned long long* arcs) {
-  RelaxRange R{front, off, off + 1, col, w, offers, nullptr, arcs, false, srcdist};
+                            const uint64_t* lend, bool heavy, const uint32_t* col, const uint32_t* w, const uint32_t* srcdist,
+                            uint32_t* offers, unsigned long long* arcs) {
+  RelaxRange R{front, off, lend, col, w, offers, nullptr, arcs, heavy, srcdist};
   return relax_binned<true>(B, R, stream);
+}
+
+int sssp_pull_binned(cudaStream_t stream, const DegreeBins& B, const uint32_t* front, const uint64_t* off, const uint64_t* lend,
+                     bool heavy, const uint32_t* col, const uint32_t* w, const uint32_t* srcdist, uint32_t* dist, uint32_t* changed,
+                     uint32_t lo, unsigned long long* counts) {
+  PullRange P{front, off, lend, col, w, dist, changed, counts, heavy, lo, srcdist};
+  return pull_binned(B, P, stream);
+}
+
+int sssp_split_rows(cudaStream_t stream, uint64_t rows, const uint64_t* off, const uint32_t* col, const uint32_t* w, uint32_t delta,
+                    uint32_t* ocol, uint32_t* ow, uint64_t* lend) {
+  if (rows) k_split_light_heavy<<<grid_for(rows * 32, 256), 256, 0, stream>>>(rows, off, col, w, delta, ocol, ow, lend);
+  GRE_LAUNCH_CHECK();
+  return GRE_SUCCESS;
 }
 
 // Changed vertices -> next queues, one lane per bitmap word (the word is cleared).  Below the
@@ -706,6 +723,7 @@ static uint64_t binned_frontier() {
   if (const char* e = getenv("GRE_SSSP_BINNED")) return strtoull(e, nullptr, 10);
   return 64;
 }
+uint64_t sssp_binned_divisor() { return binned_frontier(); }
 
 // Whether the large heavy passes pull (over the vertices that can still improve) instead of
 // pushing (along the bucket's heavy arcs), where the weights allow it (g->w32_symmetric).
@@ -714,6 +732,7 @@ static bool pull_enabled() {
   if (const char* e = getenv("GRE_SSSP_PULL")) return strtoul(e, nullptr, 10) != 0;
   return true;
 }
+bool sssp_pull_enabled() { return pull_enabled(); }
 
 // The relaxation of one frontier pass: tile starts, then k_sssp_relax over one wave of CTAs.
 int sssp_relax_tiles(cudaStream_t stream, const uint32_t* queue, uint64_t nq, const uint64_t* prefix, uint64_t total,
@@ -844,7 +863,7 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
         // the bucket's heavy arcs: only vertices at or above the limit can improve (heavy arcs
         // from the bucket land there).  (Light passes push: every unsettled vertex would have to
         // scan its light arcs at every pass of the bucket, measured slower than the push.)
-        PullRange P{front, off, lend, col, w, dist, changed, pull_counts, true, limit};
+        PullRange P{front, off, lend, col, w, dist, changed, pull_counts, true, limit, dist};
         GRE_CHECK(pull_binned(bins, P, g->stream));
         bytes += 16 * n;  // per row: its id, distance and range bounds (arcs at the end)
       } else {

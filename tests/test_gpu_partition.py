@@ -93,6 +93,26 @@ def test_partitioned_sssp_equals_oracle_and_one_gpu(P, reorder):
             assert st.traversed_edges == st1.traversed_edges
 
 
+@pytest.mark.parametrize("pull", ["0", "1"], ids=["push", "pull"])
+@pytest.mark.parametrize("binned", ["0", "4294967296"], ids=["tiles", "bins"])
+@pytest.mark.parametrize("P", [1, 3])
+def test_partitioned_sssp_forms(monkeypatch, P, binned, pull):
+    """Every relaxation form of the partitioned SSSP (arc tiles or the rank's degree bins for the
+    light offers and the pushed heavy offers, or the pulled heavy pass) on a schedule whose short
+    CTA threshold and hub chunks put rows into the CTA and chunk bins of each part."""
+    monkeypatch.setenv("GRE_ROW_SCHEDULE", "2,32,64,0")
+    monkeypatch.setenv("GRE_SSSP_BINNED", binned)
+    monkeypatch.setenv("GRE_SSSP_PULL", pull)
+    n, off, col, g = _graph(11, True, True)
+    g.set_weights_hash(WSEED)
+    R = O.Restatement.from_csr(n, off, col)
+    roots = G.sample_sources(off, 2, 6)
+    ref = R.sssp_many(roots, WSEED)
+    for i, s in enumerate(roots):
+        for dist, _ in PT.run_local(g, P, lambda part, x: part.sssp(int(s), x)):
+            np.testing.assert_array_equal(dist, ref[i])
+
+
 @pytest.mark.parametrize("P", [1, 2, 3, 4])
 @pytest.mark.parametrize("reorder", [False, True], ids=["plain", "relabelled"])
 def test_partitioned_cc_equals_oracle_and_one_gpu(P, reorder):
