@@ -341,7 +341,7 @@ void free_bins(DegreeBins& B);
 int ensure_rarc(gre_graph g);
 // Undirected edge count with both endpoints in a reached set (Graph500 TEPS numerator).
 int count_reached_edges(gre_graph g, const int32_t* level, uint64_t* edges, uint64_t rows = 1);
-// SSSP bucket width: half the mean uint32 weight (GRE_SSSP_DELTA overrides; 0 = no buckets).
+// SSSP bucket width: 3/8 of the mean uint32 weight (GRE_SSSP_DELTA overrides; 0 = no buckets).
 int sssp_delta(gre_graph g, uint32_t* delta);
 // One edge-balanced relaxation pass (sssp.cu): the frontier `queue` (nq vertices, exclusive
 // scan `prefix` of their arc counts, `total` arcs starting at base[u]) offers srcdist[u] + w to

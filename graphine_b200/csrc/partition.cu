@@ -50,7 +50,7 @@ struct gre_part_s {
   uint64_t L = 0;            // vertex slots per rank (multiple of 64)
   uint64_t arcs_in = 0, arcs_out = 0;  // arcs of the owned rows
   uint32_t* w32 = nullptr;   // weights of the out-arc rows (the graph's, when it had them)
-  uint32_t delta = 0;        // SSSP bucket width: half the mean weight (0: no buckets)
+  uint32_t delta = 0;        // SSSP bucket width: the whole graph's (sssp_delta; 0: no buckets)
   uint32_t* xof = nullptr;   // caller id -> exchange index (n)
   uint32_t* xmap = nullptr;  // exchange index -> caller id, 0xffffffff for padding (P * L)
   uint64_t cc_remote = ~0ull;  // arcs of the owned rows that lead to another rank (counted on first use)
