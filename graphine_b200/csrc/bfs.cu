@@ -29,6 +29,14 @@
 
 namespace gre {
 
+// persist.cu
+bool msbfs_persistent_available(uint64_t n);
+size_t msbfs_ctl_bytes();
+int msbfs_word_persistent(gre_graph g, unsigned long long full, unsigned long long* seen, unsigned long long* fa,
+                          unsigned long long* fb, unsigned long long* acc, uint32_t* list0, uint32_t* list1, int32_t* levels,
+                          void* ctl_mem, unsigned long long* found_per_level, uint32_t* levels_out, uint64_t* scanned,
+                          uint64_t* bytes, std::vector<unsigned long long>* found);
+
 template <class T>
 static int ws_array(gre_graph g, int slot, uint64_t count, T** p) {
   void* v = nullptr;
@@ -452,12 +460,18 @@ int gre_msbfs(gre_graph g, const uint32_t* srcs, uint32_t nsrc, int32_t* levels,
   GRE_CHECK(ws_array(g, WS_B, n, &fa));
   GRE_CHECK(ws_array(g, WS_C, n, &fb));
   unsigned long long* acc;
-  uint32_t* flist;
+  uint32_t *flist, *flist2 = nullptr;
+  unsigned char* ctl = nullptr;
   GRE_CHECK(ws_array(g, WS_D, 64, &dsrc));
   GRE_CHECK(ws_array(g, WS_E, n, &acc));
   GRE_CHECK(ws_array(g, WS_F, n, &flist));
   GRE_CHECK(ws_array(g, WS_COUNTERS, 8, &cnt));
   GRE_CHECK(ensure_bins(g, true));
+  const bool persist = msbfs_persistent_available(n);
+  if (persist) {  // the level loop as one cooperative launch per word (persist.cu)
+    GRE_CHECK(ws_array(g, WS_G, n, &flist2));
+    GRE_CHECK(ws_array(g, WS_H, msbfs_ctl_bytes(), &ctl));
+  }
   RunTimer timer(g);
   GRE_CUDA(cudaMemsetAsync(dl, 0xff, sizeof(int32_t) * nsrc * n, g->stream));
   GRE_CUDA(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * n, g->stream));
@@ -471,6 +485,16 @@ int gre_msbfs(gre_graph g, const uint32_t* srcs, uint32_t nsrc, int32_t* levels,
     GRE_CUDA(cudaMemsetAsync(fa, 0, sizeof(unsigned long long) * n, g->stream));
     int32_t* lv = dl + (uint64_t)j0 * n;
     k_ms_seed<<<1, 32, 0, g->stream>>>(dsrc, k, n, seen, fa, lv);
+    if (persist) {
+      uint32_t nl = 0;
+      std::vector<unsigned long long> found;
+      GRE_CHECK(msbfs_word_persistent(g, full, seen, fa, fb, acc, flist, flist2, lv, ctl,
+                                      (unsigned long long*)(ctl + msbfs_ctl_bytes()) - GRE_MAX_RECORDED_SUPERSTEPS, &nl,
+                                      &scanned, &bytes, nsrc <= 64 ? &found : nullptr));
+      for (unsigned long long f : found) stats_record(st, f);
+      max_levels = std::max<uint32_t>(max_levels, nl);
+      continue;
+    }
     unsigned long long* front = fa;
     unsigned long long* next = fb;
     unsigned long long live = full;  // sources whose frontier is not empty

@@ -1,0 +1,46 @@
+"""The 64-source BFS as one persistent launch (persist.cu).
+
+* The cooperative level loop gives the levels of the host-driven loop bit for bit (and the
+  oracle's), with the same per-level counts of new (source, vertex) pairs.
+* A grid-barrier wait that runs out ends the launch with GRE_TIMEOUT and leaves the context and
+  the graph usable: the budget is set to 0 (every wait fails at once; nothing faults or hangs),
+  then the same call with the default budget gives the right levels.
+"""
+import numpy as np
+import pytest
+
+import graphine_b200.gre as G
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("k", [1, 64, 70])
+def test_persistent_levels_equal_host_loop_and_oracle(monkeypatch, k):
+    n, off, col = G.rmat_host(16, 16, 31, True)
+    g = G.Graph.from_csr(n, off, col, dir=G.InOut, symmetric=True, reorder=True)
+    srcs = G.sample_sources(off, k, 4)
+    monkeypatch.setenv("GRE_PERSIST", "0")
+    host, st_host = G.msbfs(g, srcs)
+    monkeypatch.setenv("GRE_PERSIST", "1")
+    pers, st_pers = G.msbfs(g, srcs)
+    np.testing.assert_array_equal(pers, host)
+    assert st_pers.active == st_host.active and st_pers.supersteps == st_host.supersteps
+    assert st_pers.arcs_traversed == st_host.arcs_traversed
+    R = O.Restatement.from_csr(n, off, col)
+    np.testing.assert_array_equal(pers.reshape(len(srcs), n), R.bfs_many(srcs))
+
+
+def test_persistent_wait_budget_runs_out_cleanly(monkeypatch):
+    n, off, col = G.rmat_host(14, 16, 32, True)
+    g = G.Graph.from_csr(n, off, col, dir=G.InOut, symmetric=True)
+    srcs = G.sample_sources(off, 64, 5)
+    monkeypatch.setenv("GRE_PERSIST", "1")
+    monkeypatch.setenv("GRE_GRID_WAIT_MS", "0")
+    with pytest.raises(G.GreError) as e:
+        G.msbfs(g, srcs)
+    assert e.value.status == G.GRE_TIMEOUT
+    assert "grid barrier" in str(e.value)
+    monkeypatch.delenv("GRE_GRID_WAIT_MS")
+    lv, _ = G.msbfs(g, srcs)  # the same graph, the same context: a normal run
+    np.testing.assert_array_equal(lv.reshape(64, n), O.Restatement.from_csr(n, off, col).bfs_many(srcs))
