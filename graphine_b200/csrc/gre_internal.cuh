@@ -345,16 +345,17 @@ int count_reached_edges(gre_graph g, const int32_t* level, uint64_t* edges, uint
 int sssp_delta(gre_graph g, uint32_t* delta);
 // One edge-balanced relaxation pass (sssp.cu): the frontier `queue` (nq vertices, exclusive
 // scan `prefix` of their arc counts, `total` arcs starting at base[u]) offers srcdist[u] + w to
-// dist[head] (atomic min).  srcdist == dist: the one-GPU relaxation, a `changed` bit per
-// improved head; otherwise dist is a separate offer array and changed is unused.  tstart holds
+// dist[head] (atomic min), and sets the head's bit in `changed` (may be null) on improvement.
+// srcdist == dist: the one-GPU relaxation; otherwise dist is a separate offer array.  tstart holds
 // ceil(total / sssp_tile_arcs()) entries; error is set if a tile holds too many owners.
 uint64_t sssp_tile_arcs();
 // The binned form of a relaxation pass as offers (sssp.cu): every row of the bins whose bit is set
 // in `front` offers srcdist[row] + w over its light arcs [off[row], lend[row]) (heavy: [lend[row],
-// off[row+1])) into `offers` (atomic min); `arcs` (may be null) counts the arcs.
+// off[row+1])) into `offers` (atomic min), setting the entry's bit in `touched` (may be null);
+// `arcs` (may be null) counts the arcs.
 int sssp_relax_binned_offer(cudaStream_t stream, const DegreeBins& B, const uint32_t* front, const uint64_t* off,
                             const uint64_t* lend, bool heavy, const uint32_t* col, const uint32_t* w, const uint32_t* srcdist,
-                            uint32_t* offers, unsigned long long* arcs);
+                            uint32_t* offers, uint32_t* touched, unsigned long long* arcs);
 // The pull form of a pass (sssp.cu; symmetric graph with symmetric weights): every row whose
 // dist[row] >= lo takes the smallest srcdist[u] + w over its light (heavy) arcs to columns u set
 // in `front`; an improvement lowers dist[row] and sets the row's bit in `changed`.  counts[0] +=

@@ -385,6 +385,21 @@ __global__ void k_part_sssp_select(uint64_t W, uint32_t* __restrict__ pend, cons
   }
 }
 
+// Offer slots written since the last clear (bits in `touched`, one per slot of all P * L) go back
+// to "no offer", and the bits are cleared: the offer array is reset without a full memset.
+__global__ void k_part_offers_clear(uint64_t words, uint32_t* __restrict__ touched, uint32_t* __restrict__ cand) {
+  for (uint64_t wi = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; wi < words; wi += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t bits = touched[wi];
+    if (!bits) continue;
+    touched[wi] = 0;
+    while (bits) {
+      const uint32_t b = __ffs(bits) - 1;
+      bits &= bits - 1;
+      cand[(wi << 5) + b] = 0xffffffffu;
+    }
+  }
+}
+
 // arcs of the queued slots in their light ([off, lend)) or heavy ([lend, off+1)) range
 __global__ void k_part_range_degrees(const uint32_t* __restrict__ queue, uint64_t nq, const uint64_t* __restrict__ off,
                                      const uint64_t* __restrict__ lend, bool heavy, uint64_t* __restrict__ deg) {
@@ -910,6 +925,8 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
   GRE_CHECK(ws_array(s, WS_F, W, &inb));
   GRE_CHECK(ws_array(s, WS_G, P * W, &inb_all));
   GRE_CHECK(ws_array(s, WS_I, P * L, &cand));
+  uint32_t* touched;  // offer slots written since the last clear
+  GRE_CHECK(ws_array(s, WS_H, P * W, &touched));
   GRE_CHECK(ws_array(s, WS_J, P * L, &recv));
   GRE_CHECK(ws_array(s, WS_K, L + 1, &deg));
   GRE_CHECK(ws_array(s, WS_L, L + 1, &prefix));
@@ -937,6 +954,8 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
   GRE_CUDA(cudaMemsetAsync(inb, 0, sizeof(uint32_t) * W, s->stream));
   GRE_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), s->stream));
   GRE_CUDA(cudaMemsetAsync(pull_counts, 0, 2 * sizeof(unsigned long long), s->stream));
+  GRE_CUDA(cudaMemsetAsync(cand, 0xff, sizeof(uint32_t) * P * L, s->stream));  // then cleared slot by slot
+  GRE_CUDA(cudaMemsetAsync(touched, 0, sizeof(uint32_t) * P * W, s->stream));
   GRE_CUDA(cudaStreamSynchronize(s->stream));
   if (xr / L == me) {
     const uint32_t slot = xr - (uint32_t)(me * L), zero = 0, bit = 1u << (slot & 31u);
@@ -957,7 +976,6 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
   // offers of this rank's frontier `list` (or bitmap `front`, binned form) over the light or heavy
   // ranges, exchanged with the owners, who keep the smallest and mark improved slots pending
   auto offer_pass = [&](const uint32_t* list, uint64_t nlist, const uint32_t* front, uint64_t arcs, bool heavy) -> int {
-    GRE_CUDA(cudaMemsetAsync(cand, 0xff, sizeof(uint32_t) * P * L, s->stream));
     if (nlist && arcs && bdiv && nlist >= L / bdiv) {
       uint32_t* bits = const_cast<uint32_t*>(front);
       if (!bits) {  // the frontier as a bitmap, in the scan buffer (unused by this form)
@@ -966,20 +984,21 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
         k_queue_to_bits<<<grid_for(nlist, 256), 256, 0, s->stream>>>(list, nlist, bits);
         bytes += 4 * W + 4 * nlist;
       }
-      GRE_CHECK(sssp_relax_binned_offer(s->stream, B, bits, off, lend, heavy, col, w, dl, cand, nullptr));
+      GRE_CHECK(sssp_relax_binned_offer(s->stream, B, bits, off, lend, heavy, col, w, dl, cand, touched, nullptr));
       bytes += 16 * L + W * 4;  // rows scanned and their frontier bits (arcs below)
     } else if (nlist && arcs) {
       k_part_range_degrees<<<grid_for(nlist, 256), 256, 0, s->stream>>>(list, nlist, off, lend, heavy, deg);
       GRE_CUDA(cub::DeviceScan::ExclusiveSum(cubtmp, cubbytes, deg, prefix, nlist + 1, s->stream));
-      GRE_CHECK(sssp_relax_tiles(s->stream, list, nlist, prefix, arcs, tstart, heavy ? lend : off, col, w, dl, cand, nullptr,
+      GRE_CHECK(sssp_relax_tiles(s->stream, list, nlist, prefix, arcs, tstart, heavy ? lend : off, col, w, dl, cand, touched,
                                  err));
       bytes += 16 * nlist;
     }
     GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLTOALL, cand, recv, 4 * L));
+    k_part_offers_clear<<<grid_for(P * W, 256), 256, 0, s->stream>>>(P * W, touched, cand);  // after the exchange read cand
     k_part_sssp_claim<<<grid_for(L, 256), 256, 0, s->stream>>>(L, P, recv, dl, s->outdeg, pend);
     GRE_LAUNCH_CHECK();
     relaxed += arcs;
-    bytes += 12 * arcs + 4 * P * L * 3 + 4 * L;
+    bytes += 12 * arcs + 4 * P * L * 2 + 4 * P * W + 4 * L;
     return GRE_SUCCESS;
   };
   for (;;) {

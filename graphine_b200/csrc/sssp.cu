@@ -113,9 +113,9 @@ __global__ void k_tile_starts(const uint64_t* __restrict__ prefix, uint64_t nq, 
   }
 }
 
-// OFFER: the owners' distances come from srcdist and the improved heads are not recorded (the
-// partitioned path offers to a separate candidate array); otherwise from dist itself, with a
-// changed bit per improved head.
+// OFFER: the owners' distances come from srcdist and `dist` is a separate offer array (the
+// partitioned path); otherwise from dist itself.  Either way an improved entry sets its bit in
+// `changed` when that bitmap is given.
 template <bool OFFER>
 __global__ void __launch_bounds__(kTileThreads) k_sssp_relax(const uint32_t* __restrict__ queue, uint64_t nq,
                                                              const uint64_t* __restrict__ prefix, uint64_t total, const uint32_t* __restrict__ start,
@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(kTileThreads) k_sssp_relax(const uint32_t* __r
       const uint32_t nd = du[k] + wt[k];
       if (ok && nd < dv[k]) {
         atomicMin(dist + v[k], nd);
-        if (!OFFER) atomicOr(changed + (v[k] >> 5), 1u << (v[k] & 31u));
+        if (changed) atomicOr(changed + (v[k] >> 5), 1u << (v[k] & 31u));
       }
     }
     __syncthreads();
@@ -242,7 +242,7 @@ struct RelaxRange {
       for (int k = 0; k < 4; ++k)
         if (nd[k] < dv[k]) {
           atomicMin(dist + x[k], nd[k]);
-          if (!OFFER) atomicOr(changed + (x[k] >> 5), 1u << (x[k] & 31u));
+          if (changed) atomicOr(changed + (x[k] >> 5), 1u << (x[k] & 31u));
         }
     }
     for (; a < hi; a += step) {
@@ -250,7 +250,7 @@ struct RelaxRange {
       const uint32_t nd = du + __ldg(w + a);
       if (nd < __ldcg(dist + x)) {
         atomicMin(dist + x, nd);
-        if (!OFFER) atomicOr(changed + (x >> 5), 1u << (x & 31u));
+        if (changed) atomicOr(changed + (x >> 5), 1u << (x & 31u));
       }
     }
   }
@@ -527,8 +527,8 @@ __global__ void k_sssp_classes(uint64_t n, const uint64_t* __restrict__ off, con
 
 int sssp_relax_binned_offer(cudaStream_t stream, const DegreeBins& B, const uint32_t* front, const uint64_t* off,
                             const uint64_t* lend, bool heavy, const uint32_t* col, const uint32_t* w, const uint32_t* srcdist,
-                            uint32_t* offers, unsigned long long* arcs) {
-  RelaxRange R{front, off, lend, col, w, offers, nullptr, arcs, heavy, srcdist};
+                            uint32_t* offers, uint32_t* touched, unsigned long long* arcs) {
+  RelaxRange R{front, off, lend, col, w, offers, touched, arcs, heavy, srcdist};
   return relax_binned<true>(B, R, stream);
 }
 
