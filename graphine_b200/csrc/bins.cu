@@ -201,8 +201,8 @@ int build_segments(gre_graph g, DegreeBins& B, const uint64_t* off, const uint32
   if (e == cudaSuccess && nchunks) e = cudaMemcpy(B.seg_end, cend.data(), sizeof(uint64_t) * nchunks, cudaMemcpyHostToDevice);
   if (e == cudaSuccess && nchunks) e = cudaMemcpy(B.seg_slot, cslot.data(), sizeof(uint64_t) * nchunks, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cuda_status(e, "window chunk upload", __FILE__, __LINE__);
-  // partial slots the row kernels need
-  if (nchunks > B.n_hub_chunks) B.n_hub_chunks = nchunks;
+  // partial slots the row kernels need (the hub-chunk arrays keep their own count)
+  if (nchunks > B.n_partials) B.n_partials = nchunks;
   return GRE_SUCCESS;
 }
 
@@ -268,6 +268,7 @@ int build_bins(gre_graph g, DegreeBins& B, const uint64_t* off, const uint32_t* 
       }
       first.push_back(crow.size());
       B.n_hub_chunks = crow.size();
+      B.n_partials = crow.size();
       e = cudaMalloc(&B.hub_chunk_row, sizeof(uint64_t) * crow.size());
       if (e == cudaSuccess) e = cudaMalloc(&B.hub_chunk_begin, sizeof(uint64_t) * cbeg.size());
       if (e == cudaSuccess) e = cudaMalloc(&B.hub_chunk_first, sizeof(uint64_t) * first.size());
@@ -318,7 +319,7 @@ int degree_key(gre_graph g, const uint64_t* off, std::string* key) {
 // Times `reps` probe supersteps under the current bins; returns the fastest, in ms.
 int probe(gre_graph g, const DegreeBins& B, const uint64_t* off, const uint32_t* col, const double* x, double* y, float* best_ms) {
   double* partial = nullptr;
-  GRE_CUDA(cudaMalloc(&partial, sizeof(double) * (B.n_hub_chunks + 1)));
+  GRE_CUDA(cudaMalloc(&partial, sizeof(double) * (B.n_partials + 1)));
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaError_t e = cudaEventCreate(&e0);
   if (e == cudaSuccess) e = cudaEventCreate(&e1);

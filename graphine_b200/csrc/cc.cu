@@ -149,7 +149,7 @@ int gre_cc(gre_graph g, uint32_t* label, gre_stats* st) {
   GRE_CHECK(perm_out_begin(g, dfinal, 1, 4, (void**)&dl));
   GRE_CHECK(g->ws.get(WS_A, sizeof(uint32_t) * n, &p));
   parent = (uint32_t*)p;
-  GRE_CHECK(g->ws.get(WS_B, sizeof(double) * (g->bins_out.n_hub_chunks + 1), &p));
+  GRE_CHECK(g->ws.get(WS_B, sizeof(double) * (g->bins_out.n_partials + 1), &p));
   partial = (double*)p;
   constexpr uint32_t kSampled = 2, kSample = 1024;
   uint32_t *skip = nullptr, *sample = nullptr;

@@ -84,7 +84,9 @@ struct DegreeBins {
   uint64_t count[NB] = {};
   uint64_t start[NB] = {};   // offsets into `rows`
   uint32_t* rows = nullptr;  // row ids grouped by bin (device)
-  uint64_t n_hub_chunks = 0; // chunks of the multi-CTA bin
+  uint64_t n_hub_chunks = 0; // chunks of the multi-CTA bin (entries of hub_chunk_row / _begin)
+  uint64_t n_partials = 0;   // partial-sum slots the row kernels need: the hub chunks, or the
+                             // window chunks when the schedule splits rows by source window
   uint64_t* hub_chunk_row = nullptr;   // per chunk: index into the multi-CTA bin
   uint64_t* hub_chunk_begin = nullptr; // per chunk: first arc
   uint64_t* hub_chunk_first = nullptr; // per multi-CTA row: first chunk id (size count+1)

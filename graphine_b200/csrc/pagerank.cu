@@ -395,7 +395,7 @@ static int weighted_prep(gre_graph g, WeightedPrep* wp) {
   GRE_CHECK(ws_array(g, WS_J, g->m, &wp->p));
   GRE_CHECK(ws_array(g, WS_K, g->m, &wp->pw));
   double* partial;
-  GRE_CHECK(ws_array(g, WS_H, g->bins_out.n_hub_chunks + 1, &partial));
+  GRE_CHECK(ws_array(g, WS_H, g->bins_out.n_partials + 1, &partial));
   GRE_CUDA(cudaMemsetAsync(wp->s, 0, sizeof(double) * g->n, g->stream));
   GRE_CHECK(rows::reduce_rows(g->bins_out, g->off, GatherW{g->w64}, FinishStore{wp->s}, partial, g->stream));
   k_csr_normalise<<<grid_for(g->n * 32, 256), 256, 0, g->stream>>>(g->n, g->off, g->w64, wp->s, wp->p);
@@ -410,7 +410,7 @@ static int affine_solve(gre_graph g, const DegreeBins& B, const uint64_t* off, c
                         double* xa, double* xb, double** result, uint32_t* iters_done, gre_stats* st) {
   double* partial;
   double* maxdiff;
-  GRE_CHECK(ws_array(g, WS_H, B.n_hub_chunks + 1, &partial));
+  GRE_CHECK(ws_array(g, WS_H, B.n_partials + 1, &partial));
   GRE_CHECK(ws_array(g, WS_COUNTERS, 2, &maxdiff));
   k_affine_init<<<grid_for(g->n, 256), 256, 0, g->stream>>>(g->n, base, base_c, scale, xa, xb);
   // one iteration x -> y; maxdiff holds that iteration's largest change (reset first)
@@ -471,7 +471,7 @@ int gre_pagerank(gre_graph g, int variant, double d, uint32_t iters, double* pr,
   GRE_CHECK(perm_out_begin(g, dout, 1, 8, (void**)&dpr));
   GRE_CHECK(ws_array(g, WS_A, n, &c0));
   GRE_CHECK(ws_array(g, WS_B, n, &c1));
-  GRE_CHECK(ws_array(g, WS_C, g->bins_in.n_hub_chunks + 1, &partial));
+  GRE_CHECK(ws_array(g, WS_C, g->bins_in.n_partials + 1, &partial));
   const double tele = 1.0 - d;
   const bool refresh = variant == GRE_PR_ITER;
   RunTimer timer(g);
@@ -532,7 +532,7 @@ int gre_ppr(gre_graph g, const uint32_t* seeds, uint32_t k, double d, uint32_t i
     double *c0, *c1, *partial;
     GRE_CHECK(ws_array(g, WS_A, n, &c0));
     GRE_CHECK(ws_array(g, WS_B, n, &c1));
-    GRE_CHECK(ws_array(g, WS_C, g->bins_in.n_hub_chunks + 1, &partial));
+    GRE_CHECK(ws_array(g, WS_C, g->bins_in.n_partials + 1, &partial));
     for (uint32_t j = 0; j < k; ++j) {
       double* x = dout + (uint64_t)j * n;
       k_ppr1_init<<<grid_for(n, 256), 256, 0, g->stream>>>(n, hs[j], g->outdeg, tele, x, c0, c1);
@@ -671,7 +671,7 @@ int gre_pagerank_adjoint(gre_graph g, double d, const double* r, const double* c
   GRE_CHECK(affine_solve(g, g->bins_out, g->off, g->col, wp.p, dc, 1.0, 0.0, d, tol, max_iters, xa, xb, &res, &done, st));
   // pl[u] = sum_k P_uk lambda_k (rows without arcs keep 0)
   double* partial;
-  GRE_CHECK(ws_array(g, WS_H, g->bins_out.n_hub_chunks + 1, &partial));
+  GRE_CHECK(ws_array(g, WS_H, g->bins_out.n_partials + 1, &partial));
   GRE_CUDA(cudaMemsetAsync(pl, 0, sizeof(double) * n, g->stream));
   GRE_CHECK(rows::reduce_rows(g->bins_out, g->off, GatherWeighted{g->col, wp.p, res}, FinishStore{pl}, partial, g->stream));
   k_grad_w<<<grid_for(n * 32, 256), 256, 0, g->stream>>>(n, g->off, g->col, dr, wp.s, res, pl, d, dgw);

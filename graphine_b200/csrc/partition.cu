@@ -856,7 +856,7 @@ int gre_part_pagerank(gre_part p, int variant, double d, uint32_t iters, double*
   GRE_CHECK(ws_array(s, WS_B, P * L, &pr_all));
   GRE_CHECK(ws_array(s, WS_C, L, &contrib));
   GRE_CHECK(ws_array(s, WS_D, P * L, &contrib_all));
-  GRE_CHECK(ws_array(s, WS_E, s->bins_in.n_hub_chunks + 1, &partial));
+  GRE_CHECK(ws_array(s, WS_E, s->bins_in.n_partials + 1, &partial));
   GRE_CHECK(prepare_output(s, pr, n, WS_OUTBUF, &dout));
   const double tele = 1.0 - d;
   const bool refresh = variant == GRE_PR_ITER;
@@ -1106,7 +1106,7 @@ int gre_part_cc(gre_part p, uint32_t* label, gre_exchange_fn xchg, void* ctx, gr
   GRE_CHECK(ws_array(s, WS_C, L, &parent));
   GRE_CHECK(ws_array(s, WS_D, L, &rootlab));
   GRE_CHECK(ws_array(s, WS_E, ((L + 31) >> 5) + kSample, &skip));
-  GRE_CHECK(ws_array(s, WS_F, std::max(s->bins_in.n_hub_chunks, s->bins_out.n_hub_chunks) + 1, &partial));
+  GRE_CHECK(ws_array(s, WS_F, std::max(s->bins_in.n_partials, s->bins_out.n_partials) + 1, &partial));
   GRE_CHECK(ws_array(s, WS_COUNTERS, 2, &c));
   GRE_CHECK(ws_array(s, WS_OUTBUF2, P, &call));
   GRE_CHECK(prepare_output(s, label, n, WS_OUTBUF, &dout));

@@ -139,7 +139,7 @@ __global__ void k_rows_chunk_finish(const uint32_t* __restrict__ rows, uint64_t 
   }
 }
 
-// Launch the reductions of every non-empty row.  `partial` holds bins.n_hub_chunks doubles.
+// Launch the reductions of every non-empty row.  `partial` holds bins.n_partials doubles.
 template <class Gather, class Finish>
 int reduce_rows(const DegreeBins& B, const uint64_t* off, Gather gat, Finish fin, double* partial, cudaStream_t s) {
   const uint32_t* r = B.rows;

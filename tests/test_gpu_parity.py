@@ -408,6 +408,14 @@ def test_forced_row_schedules_match_oracle(monkeypatch, schedule, directed):
     if not directed:
         lab, _ = G.cc(g)
         np.testing.assert_array_equal(lab, R.cc()[0])
+    # SSSP with every pass through the bins (CTA rows and hub chunks, under window schedules too)
+    monkeypatch.setenv("GRE_SSSP_BINNED", "4294967296")
+    g.set_weights_hash(6)
+    roots = G.sample_sources(off, 2, 7)
+    ref = R.sssp_many(roots, 6)
+    for pull in ("0", "1"):
+        monkeypatch.setenv("GRE_SSSP_PULL", pull)
+        np.testing.assert_array_equal(G.sssp(g, roots)[0].reshape(2, n), ref)
     w = np.exp(np.random.default_rng(3).standard_normal(len(col)))
     g.set_weights_f64(w)
     r1, _, _ = G.pagerank_weighted(g, 0.85, None, tol=1e-14, max_iters=500)
