@@ -415,6 +415,42 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
   base = __shfl_sync(0xffffffffu, base, leader);
   return want ? base + __popc(mask & ((1u << lane) - 1u)) : 0xffffffffu;
 }
+
+// Per-warp staging of appends to K global lists.  A pass that appends most of the graph through
+// warp_append makes one global atomic per 32 items on the same few counters, and those atomics
+// bound it; here each warp gathers its items in shared memory (CAP per list) and moves them out
+// with one atomic per CAP items and coalesced stores.  Every call is warp-uniform (all 32 lanes,
+// the same k); `buf` is this warp's K * CAP words of shared memory.  The order of items in a
+// list is not kept (callers treat lists as sets).
+template <int K, int CAP>
+struct WarpLists {
+  uint32_t* buf;
+  uint32_t held[K];
+  __device__ __forceinline__ explicit WarpLists(uint32_t* b) : buf(b) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) held[k] = 0;
+  }
+  template <int k>
+  __device__ __forceinline__ void push(bool want, uint32_t v, uint32_t* counter, uint32_t* list) {
+    const uint32_t mask = __ballot_sync(0xffffffffu, want);
+    if (!mask) return;
+    if (held[k] + 32 > CAP) flush<k>(counter, list);
+    if (want) buf[k * CAP + held[k] + __popc(mask & ((1u << lane_id()) - 1u))] = v;
+    held[k] += __popc(mask);
+  }
+  template <int k>
+  __device__ __forceinline__ void flush(uint32_t* counter, uint32_t* list) {
+    __syncwarp();
+    const uint32_t c = held[k];
+    if (!c) return;
+    uint32_t base = 0;
+    if (lane_id() == 0) base = atomicAdd(counter, c);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    for (uint32_t i = lane_id(); i < c; i += 32) list[base + i] = buf[k * CAP + i];
+    __syncwarp();
+    held[k] = 0;
+  }
+};
 #endif
 
 }  // namespace gre

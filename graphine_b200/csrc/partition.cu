@@ -333,9 +333,11 @@ struct SsspCounters {
   unsigned long long pad[3];
 };
 
-__global__ void k_part_sssp_select(uint64_t W, uint32_t* __restrict__ pend, const uint32_t* __restrict__ dist, uint32_t limit,
+__global__ void __launch_bounds__(256) k_part_sssp_select(uint64_t W, uint32_t* __restrict__ pend, const uint32_t* __restrict__ dist, uint32_t limit,
                                    const uint64_t* __restrict__ off, const uint64_t* __restrict__ lend, uint32_t* __restrict__ inb,
                                    uint32_t* __restrict__ queue, SsspCounters* __restrict__ c) {
+  __shared__ uint32_t stage[8][1024];
+  WarpLists<1, 1024> out(stage[threadIdx.x >> 5]);
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   unsigned long long left = 0, arcs = 0, joined = 0;
   uint32_t dmin = 0xffffffffu;
@@ -362,8 +364,7 @@ __global__ void k_part_sssp_select(uint64_t W, uint32_t* __restrict__ pend, cons
           dmin = min(dmin, d);
         }
       }
-      const uint32_t pos = warp_append((uint32_t*)&c->near, take);
-      if (take) queue[pos] = i;
+      out.push<0>(take, i, (uint32_t*)&c->near, queue);
     }
     if (w < W && pend[w] != keep) pend[w] = keep;
     if (join) {
@@ -371,6 +372,7 @@ __global__ void k_part_sssp_select(uint64_t W, uint32_t* __restrict__ pend, cons
       joined += __popc(join);
     }
   }
+  out.flush<0>((uint32_t*)&c->near, queue);
   dmin = __reduce_min_sync(0xffffffffu, dmin);
   for (int o = 16; o > 0; o >>= 1) {
     left += __shfl_xor_sync(0xffffffffu, left, o);
@@ -396,6 +398,76 @@ __global__ void k_part_offers_clear(uint64_t words, uint32_t* __restrict__ touch
       const uint32_t b = __ffs(bits) - 1;
       bits &= bits - 1;
       cand[(wi << 5) + b] = 0xffffffffu;
+    }
+  }
+}
+
+// The offers of one superstep as per-owner lists, for a superstep whose offers are few: owner q's
+// block (`block` uint2 from send + q * block) holds its count in .x of the first element, then
+// (slot within q's part, distance) pairs of the offer slots written since the last clear.  The
+// slots go back to "no offer" and their bits are cleared, as k_part_offers_clear.  The offers of
+// a superstep are at most its arcs, the bound the host sizes `cap` by; a pair past `cap` would
+// set *err and be dropped.  grid.y = owner; a warp appends its 32 words' pairs with one atomic.
+__global__ void k_part_offers_pack(uint64_t W, uint32_t* __restrict__ touched, uint32_t* __restrict__ cand,
+                                   uint2* __restrict__ send, uint64_t block, uint64_t cap, uint32_t* __restrict__ err) {
+  const uint64_t q = blockIdx.y;
+  uint32_t* tq = touched + q * W;
+  uint32_t* cq = cand + q * W * 32;
+  uint2* out = send + q * block;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) & ~31ull; base < W; base += stride) {
+    const uint64_t wi = base + lane;
+    uint32_t bits = wi < W ? tq[wi] : 0u;
+    if (!__any_sync(0xffffffffu, bits != 0)) continue;
+    const uint32_t k = __popc(bits);
+    uint32_t incl = k;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= (uint32_t)o) incl += t;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    uint32_t at = 0;
+    if (lane == 0) at = atomicAdd(&out[0].x, total);
+    at = __shfl_sync(0xffffffffu, at, 0) + incl - k;
+    if (bits) tq[wi] = 0;
+    while (bits) {
+      const uint32_t b = __ffs(bits) - 1;
+      bits &= bits - 1;
+      const uint32_t slot = (uint32_t)(wi << 5) + b;
+      if (at < cap) {
+        out[1 + at] = make_uint2(slot, cq[slot]);
+      } else {
+        atomicOr(err, 2u);
+      }
+      cq[slot] = 0xffffffffu;
+      ++at;
+    }
+  }
+}
+
+// SSSP claim from per-owner lists (k_part_offers_pack's blocks, one from each rank): the distance
+// of each offered slot becomes the smallest of its offers and an improved slot with out-arcs is
+// marked pending, as k_part_sssp_claim does from the dense offer arrays.  A count above `cap` or
+// a slot past L (never written by the pack) sets *err and is not read.
+__global__ void k_part_sssp_claim_lists(uint64_t P, uint64_t L, const uint2* __restrict__ recv, uint64_t block, uint64_t cap,
+                                        uint32_t* __restrict__ dist, const uint32_t* __restrict__ outdeg,
+                                        uint32_t* __restrict__ pend, uint32_t* __restrict__ err) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t q = 0; q < P; ++q) {
+    const uint2* in = recv + q * block;
+    uint64_t cnt = in[0].x;
+    if (cnt > cap) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(err, 2u);
+      cnt = cap;
+    }
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < cnt; i += stride) {
+      const uint2 o = in[1 + i];
+      if (o.x >= L) {
+        atomicOr(err, 2u);
+        continue;
+      }
+      if (o.y < atomicMin(dist + o.x, o.y) && outdeg[o.x]) atomicOr(pend + (o.x >> 5), 1u << (o.x & 31u));
     }
   }
 }
@@ -887,6 +959,14 @@ int gre_part_pagerank(gre_part p, int variant, double d, uint32_t iters, double*
   return GRE_SUCCESS;
 }
 
+// A light superstep's offers travel as per-owner lists when (its most offers + 1) * d <= L, d from
+// GRE_PART_SPARSE (default 8: lists of at most an eighth of the dense exchange's bytes); 0 keeps
+// the dense exchange for every superstep.
+static uint64_t part_sparse_offers() {
+  if (const char* e = getenv("GRE_PART_SPARSE")) return strtoull(e, nullptr, 10);
+  return 8;
+}
+
 int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg, void* ctx, gre_stats* st) {
   if (!p || !dist || !xchg) return GRE_NULL;
   gre_graph s = p->sub;
@@ -945,6 +1025,7 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
   GRE_CHECK(s->ws.get(WS_CUB, cubbytes, &cubtmp));
   const uint64_t bdiv = sssp_binned_divisor();
   const bool pull = p->w_sym && delta && sssp_pull_enabled();
+  const uint64_t sparse = part_sparse_offers();
 
   RunTimer timer(s);
   uint32_t xr = 0;
@@ -975,7 +1056,11 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
   std::vector<SsspCounters> h(P);
   // offers of this rank's frontier `list` (or bitmap `front`, binned form) over the light or heavy
   // ranges, exchanged with the owners, who keep the smallest and mark improved slots pending
-  auto offer_pass = [&](const uint32_t* list, uint64_t nlist, const uint32_t* front, uint64_t arcs, bool heavy) -> int {
+  // `cap` > 0: every rank's offers of this pass are at most cap, and they travel as per-owner
+  // (slot, distance) lists of cap pairs (in the gather buffer, unused by light supersteps) instead
+  // of the dense P * L offer arrays
+  auto offer_pass = [&](const uint32_t* list, uint64_t nlist, const uint32_t* front, uint64_t arcs, bool heavy,
+                        uint64_t cap) -> int {
     if (nlist && arcs && bdiv && nlist >= L / bdiv) {
       uint32_t* bits = const_cast<uint32_t*>(front);
       if (!bits) {  // the frontier as a bitmap, in the scan buffer (unused by this form)
@@ -993,12 +1078,25 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
                                  err));
       bytes += 16 * nlist;
     }
-    GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLTOALL, cand, recv, 4 * L));
-    k_part_offers_clear<<<grid_for(P * W, 256), 256, 0, s->stream>>>(P * W, touched, cand);  // after the exchange read cand
-    k_part_sssp_claim<<<grid_for(L, 256), 256, 0, s->stream>>>(L, P, recv, dl, s->outdeg, pend);
+    if (cap) {
+      const uint64_t block = cap + 1;  // uint2: the count, then the pairs
+      uint2* send = (uint2*)dist_all;
+      GRE_CUDA(cudaMemset2DAsync(send, 8 * block, 0, 8, P, s->stream));
+      const dim3 grid((unsigned)std::min<uint64_t>(grid_for(W, 256), 4 * 148), (unsigned)P);
+      k_part_offers_pack<<<grid, 256, 0, s->stream>>>(W, touched, cand, send, block, cap, err);
+      GRE_LAUNCH_CHECK();
+      GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLTOALL, send, recv, 8 * block));
+      k_part_sssp_claim_lists<<<grid_for(cap, 256, 4), 256, 0, s->stream>>>(P, L, (const uint2*)recv, block, cap, dl,
+                                                                             s->outdeg, pend, err);
+      bytes += 12 * arcs + 4 * P * W + 8 * P * block * 2;
+    } else {
+      GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLTOALL, cand, recv, 4 * L));
+      k_part_offers_clear<<<grid_for(P * W, 256), 256, 0, s->stream>>>(P * W, touched, cand);  // after the exchange read cand
+      k_part_sssp_claim<<<grid_for(L, 256), 256, 0, s->stream>>>(L, P, recv, dl, s->outdeg, pend);
+      bytes += 12 * arcs + 4 * P * L * 2 + 4 * P * W + 4 * L;
+    }
     GRE_LAUNCH_CHECK();
     relaxed += arcs;
-    bytes += 12 * arcs + 4 * P * L * 2 + 4 * P * W + 4 * L;
     return GRE_SUCCESS;
   };
   for (;;) {
@@ -1018,7 +1116,10 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
     }
     bytes += 4 * W + 8 * (h[me].near + h[me].pending);
     if (near) {  // a light superstep
-      GRE_CHECK(offer_pass(queue, h[me].near, nullptr, h[me].arcs, false));
+      uint64_t most = 0;  // the most offers any rank can make (the same on every rank)
+      for (const SsspCounters& x : h) most = std::max<uint64_t>(most, x.arcs);
+      const uint64_t cap = sparse && (most + 1) * sparse <= L && 2 * (most + 1) <= L ? std::max<uint64_t>(most, 1) : 0;
+      GRE_CHECK(offer_pass(queue, h[me].near, nullptr, h[me].arcs, false, cap));
       ++steps;
       stats_record(st, near);
       continue;
@@ -1047,7 +1148,7 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
             GRE_CUDA(cudaStreamSynchronize(s->stream));
           }
         }
-        GRE_CHECK(offer_pass(queue, nb, inb, arcs, true));
+        GRE_CHECK(offer_pass(queue, nb, inb, arcs, true, 0));
       }
       GRE_CUDA(cudaMemsetAsync(inb, 0, sizeof(uint32_t) * W, s->stream));
       bucket = 0;
@@ -1074,7 +1175,7 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
   GRE_CUDA(cudaMemcpyAsync(pc, pull_counts, sizeof pc, cudaMemcpyDeviceToHost, s->stream));
   GRE_CUDA(cudaStreamSynchronize(s->stream));
   if (herr) {
-    set_error("gre_part_sssp: frontier tile overflow");
+    set_error(herr & 1u ? "gre_part_sssp: frontier tile overflow" : "gre_part_sssp: offer list overflow");
     return GRE_FAILURE;
   }
   GRE_CHECK(finish_output(s, dist, dout, n));

@@ -550,10 +550,14 @@ int sssp_split_rows(cudaStream_t stream, uint64_t rows, const uint64_t* off, con
 // limit a vertex joins the near queue if it has light arcs, and the bucket list (once per
 // bucket) if it has heavy arcs; its far entry, if any, becomes void.  At or above the limit it
 // joins the far pile unless already there.  Vertices without out-arcs are dropped.
-__global__ void k_sssp_classify(uint64_t nwords, uint32_t* __restrict__ changed, const uint32_t* __restrict__ dist,
+constexpr int kStage = 512;  // items per list that a warp stages in shared memory (3 lists x 8 warps: 48 KB)
+
+__global__ void __launch_bounds__(256) k_sssp_classify(uint64_t nwords, uint32_t* __restrict__ changed, const uint32_t* __restrict__ dist,
                                 const uint32_t* __restrict__ lbits, const uint32_t* __restrict__ hbits, uint32_t near_limit,
                                 uint32_t* __restrict__ near, uint32_t* __restrict__ infar, uint32_t* __restrict__ far,
                                 uint32_t* __restrict__ inbucket, uint32_t* __restrict__ blist, uint32_t* __restrict__ counters) {
+  __shared__ uint32_t stage[8][3 * kStage];
+  WarpLists<3, kStage> out(stage[threadIdx.x >> 5]);
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t base = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) & ~31ull; base < nwords; base += stride) {
     const uint64_t wi = base + (threadIdx.x & 31u);
@@ -591,16 +595,16 @@ __global__ void k_sssp_classify(uint64_t nwords, uint32_t* __restrict__ changed,
           }
         }
       }
-      const uint32_t p = warp_append(counters, to_near);
-      if (to_near) near[p] = v;
-      const uint32_t f = warp_append(counters + 2, to_far);
-      if (to_far) far[f] = v;
-      const uint32_t q = warp_append(counters + 4, to_bucket);
-      if (to_bucket) blist[q] = v;
+      out.push<0>(to_near, v, counters, near);
+      out.push<1>(to_far, v, counters + 2, far);
+      out.push<2>(to_bucket, v, counters + 4, blist);
     }
     if (set_far | clear_far) infar[wi] = (fbits | set_far) & ~clear_far;  // one lane owns the word
     if (set_bucket) inbucket[wi] = bbits | set_bucket;
   }
+  out.flush<0>(counters, near);
+  out.flush<1>(counters + 2, far);
+  out.flush<2>(counters + 4, blist);
 }
 
 // The bucket's heavy arcs have been relaxed: its members leave the bucket list.
@@ -628,10 +632,12 @@ __global__ void k_sssp_seed(uint32_t src, const uint64_t* __restrict__ off, cons
 // queue and the bucket list (as in k_sssp_classify; their far bit is cleared), the others stay;
 // entries whose far bit was cleared (the vertex went to the near queue since) are dropped.
 // counters[3] gets the smallest distance left.
-__global__ void k_far_split(const uint32_t* __restrict__ far, uint64_t nfar, const uint32_t* __restrict__ dist, uint32_t near_limit,
+__global__ void __launch_bounds__(256) k_far_split(const uint32_t* __restrict__ far, uint64_t nfar, const uint32_t* __restrict__ dist, uint32_t near_limit,
                             const uint32_t* __restrict__ lbits, const uint32_t* __restrict__ hbits, uint32_t* __restrict__ infar,
                             uint32_t* __restrict__ near, uint32_t* __restrict__ far_out, uint32_t* __restrict__ inbucket,
                             uint32_t* __restrict__ blist, uint32_t* __restrict__ counters) {
+  __shared__ uint32_t stage[8][3 * kStage];
+  WarpLists<3, kStage> out(stage[threadIdx.x >> 5]);
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   uint32_t dmin = 0xffffffffu;
   for (uint64_t base = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) & ~31ull; base < nfar; base += stride) {
@@ -653,13 +659,13 @@ __global__ void k_far_split(const uint32_t* __restrict__ far, uint64_t nfar, con
         }
       }
     }
-    const uint32_t p = warp_append(counters, to_near);
-    if (to_near) near[p] = v;
-    const uint32_t k = warp_append(counters + 2, keep);
-    if (keep) far_out[k] = v;
-    const uint32_t q = warp_append(counters + 4, to_bucket);
-    if (to_bucket) blist[q] = v;
+    out.push<0>(to_near, v, counters, near);
+    out.push<1>(keep, v, counters + 2, far_out);
+    out.push<2>(to_bucket, v, counters + 4, blist);
   }
+  out.flush<0>(counters, near);
+  out.flush<1>(counters + 2, far_out);
+  out.flush<2>(counters + 4, blist);
   dmin = __reduce_min_sync(0xffffffffu, dmin);
   if ((threadIdx.x & 31u) == 0 && dmin != 0xffffffffu) atomicMin(counters + 3, dmin);
 }
@@ -750,7 +756,7 @@ int sssp_relax_tiles(cudaStream_t stream, const uint32_t* queue, uint64_t nq, co
     k_sssp_relax<false><<<grid, kTileThreads, 0, stream>>>(queue, nq, prefix, total, tstart, base, col, w, nullptr, dist, changed,
                                                            error);
   else
-    k_sssp_relax<true><<<grid, kTileThreads, 0, stream>>>(queue, nq, prefix, total, tstart, base, col, w, srcdist, dist, nullptr,
+    k_sssp_relax<true><<<grid, kTileThreads, 0, stream>>>(queue, nq, prefix, total, tstart, base, col, w, srcdist, dist, changed,
                                                           error);
   GRE_LAUNCH_CHECK();
   return GRE_SUCCESS;
@@ -871,7 +877,7 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
         RelaxRange R{front, off, lend, col, w, dist, changed, binned_arcs, heavy, nullptr};
         GRE_CHECK(relax_binned<false>(bins, R, g->stream));
       }
-      k_sssp_classify<<<grid_for(nwords, 256, 8), 256, 0, g->stream>>>(nwords, changed, dist, lbits, hbits, limit, out_near, infar,
+      k_sssp_classify<<<grid_for(nwords, 256, 4), 256, 0, g->stream>>>(nwords, changed, dist, lbits, hbits, limit, out_near, infar,
                                                                         far, inbucket, blist, cnt);
       GRE_LAUNCH_CHECK();
       GRE_CHECK(read_counters());
@@ -891,7 +897,7 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
     if (total) {
       GRE_CHECK(sssp_relax_tiles(g->stream, list, nlist, prefix, total, tstart, heavy ? lend : off, col, w, dist, dist, changed,
                                  cnt + 1));
-      k_sssp_classify<<<grid_for(nwords, 256, 8), 256, 0, g->stream>>>(nwords, changed, dist, lbits, hbits, limit, out_near, infar,
+      k_sssp_classify<<<grid_for(nwords, 256, 4), 256, 0, g->stream>>>(nwords, changed, dist, lbits, hbits, limit, out_near, infar,
                                                                         far, inbucket, blist, cnt);
     }
     GRE_LAUNCH_CHECK();
@@ -938,7 +944,7 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
       if (p == 0) limit = limit > 0xffffffffu - delta ? 0xffffffffu : limit + delta;
       else limit = lowest > 0xffffffffu - delta ? 0xffffffffu : lowest + delta;
       GRE_CHECK(init_counters(g, cnt, 0, 0, 0));
-      k_far_split<<<grid_for(nfar, 256, 8), 256, 0, g->stream>>>(far, nfar, dist, limit, lbits, hbits, infar, q, far2, inbucket,
+      k_far_split<<<grid_for(nfar, 256, 4), 256, 0, g->stream>>>(far, nfar, dist, limit, lbits, hbits, infar, q, far2, inbucket,
                                                                   blist, cnt);
       GRE_LAUNCH_CHECK();
       GRE_CHECK(read_counters());

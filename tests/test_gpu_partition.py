@@ -93,16 +93,20 @@ def test_partitioned_sssp_equals_oracle_and_one_gpu(P, reorder):
             assert st.traversed_edges == st1.traversed_edges
 
 
+@pytest.mark.parametrize("sparse", ["0", "1"], ids=["dense", "lists"])
 @pytest.mark.parametrize("pull", ["0", "1"], ids=["push", "pull"])
 @pytest.mark.parametrize("binned", ["0", "4294967296"], ids=["tiles", "bins"])
 @pytest.mark.parametrize("P", [1, 3])
-def test_partitioned_sssp_forms(monkeypatch, P, binned, pull):
+def test_partitioned_sssp_forms(monkeypatch, P, binned, pull, sparse):
     """Every relaxation form of the partitioned SSSP (arc tiles or the rank's degree bins for the
-    light offers and the pushed heavy offers, or the pulled heavy pass) on a schedule whose short
-    CTA threshold and hub chunks put rows into the CTA and chunk bins of each part."""
+    light offers and the pushed heavy offers, or the pulled heavy pass; light offers exchanged as
+    dense per-owner arrays, or as (slot, distance) lists whenever they fit half the dense bytes)
+    on a schedule whose short CTA threshold and hub chunks put rows into the CTA and chunk bins
+    of each part."""
     monkeypatch.setenv("GRE_ROW_SCHEDULE", "2,32,64,0")
     monkeypatch.setenv("GRE_SSSP_BINNED", binned)
     monkeypatch.setenv("GRE_SSSP_PULL", pull)
+    monkeypatch.setenv("GRE_PART_SPARSE", sparse)
     n, off, col, g = _graph(11, True, True)
     g.set_weights_hash(WSEED)
     R = O.Restatement.from_csr(n, off, col)
