@@ -39,7 +39,7 @@ int cuda_status(cudaError_t e, const char* what, const char* file, int line);
 // until the handle is freed, so repeated runs do no allocation.
 // ---------------------------------------------------------------------------------------------
 enum WsSlot {
-  WS_A = 0, WS_B, WS_C, WS_D, WS_E, WS_F, WS_G, WS_H, WS_I, WS_J, WS_K, WS_L,
+  WS_A = 0, WS_B, WS_C, WS_D, WS_E, WS_F, WS_G, WS_H, WS_I, WS_J, WS_K, WS_L, WS_M,
   WS_COUNTERS,   // small per-run counters (device-side)
   WS_CUB,        // CUB temporary storage
   WS_OUTBUF,     // device staging of results bound for host memory
@@ -345,19 +345,32 @@ int ensure_rarc(gre_graph g);
 int count_reached_edges(gre_graph g, const int32_t* level, uint64_t* edges, uint64_t rows = 1);
 // SSSP bucket width: 3/8 of the mean uint32 weight (GRE_SSSP_DELTA overrides; 0 = no buckets).
 int sssp_delta(gre_graph g, uint32_t* delta);
+// Heads a partitioned relaxation owns itself (sssp.cu offer forms): heads in [lo, lo + len) are
+// relaxed in place, as in the one-GPU pass (dist[head - lo] lowered by atomic min, the head's bit
+// set in `pend` when it has out-arcs); only the other heads are offered.  len = 0: none.
+struct OwnHeads {
+  uint64_t lo = 0, len = 0;
+  uint32_t* dist = nullptr;
+  uint32_t* pend = nullptr;
+  const uint32_t* outdeg = nullptr;
+};
 // One edge-balanced relaxation pass (sssp.cu): the frontier `queue` (nq vertices, exclusive
 // scan `prefix` of their arc counts, `total` arcs starting at base[u]) offers srcdist[u] + w to
 // dist[head] (atomic min), and sets the head's bit in `changed` (may be null) on improvement.
-// srcdist == dist: the one-GPU relaxation; otherwise dist is a separate offer array.  tstart holds
-// ceil(total / sssp_tile_arcs()) entries; error is set if a tile holds too many owners.
+// srcdist == dist: the one-GPU relaxation; otherwise dist is a separate offer array, an offer at
+// or above known[head] (an upper bound of the head's distance; may be null) is dropped, and the
+// heads in `own` are relaxed in place.  tstart holds ceil(total / sssp_tile_arcs()) entries;
+// error is set if a tile holds too many owners.
 uint64_t sssp_tile_arcs();
 // The binned form of a relaxation pass as offers (sssp.cu): every row of the bins whose bit is set
 // in `front` offers srcdist[row] + w over its light arcs [off[row], lend[row]) (heavy: [lend[row],
 // off[row+1])) into `offers` (atomic min), setting the entry's bit in `touched` (may be null);
-// `arcs` (may be null) counts the arcs.
+// offers at or above known[head] (may be null) are dropped, the heads in `own` are relaxed in
+// place; `arcs` (may be null) counts the arcs.
 int sssp_relax_binned_offer(cudaStream_t stream, const DegreeBins& B, const uint32_t* front, const uint64_t* off,
                             const uint64_t* lend, bool heavy, const uint32_t* col, const uint32_t* w, const uint32_t* srcdist,
-                            uint32_t* offers, uint32_t* touched, unsigned long long* arcs);
+                            uint32_t* offers, uint32_t* touched, const uint32_t* known, const OwnHeads& own,
+                            unsigned long long* arcs);
 // The pull form of a pass (sssp.cu; symmetric graph with symmetric weights): every row whose
 // dist[row] >= lo takes the smallest srcdist[u] + w over its light (heavy) arcs to columns u set
 // in `front`; an improvement lowers dist[row] and sets the row's bit in `changed`.  counts[0] +=
@@ -374,7 +387,7 @@ uint64_t sssp_binned_divisor();
 bool sssp_pull_enabled();
 int sssp_relax_tiles(cudaStream_t stream, const uint32_t* queue, uint64_t nq, const uint64_t* prefix, uint64_t total,
                      uint32_t* tstart, const uint64_t* base, const uint32_t* col, const uint32_t* w, const uint32_t* srcdist,
-                     uint32_t* dist, uint32_t* changed, uint32_t* error);
+                     uint32_t* dist, uint32_t* changed, uint32_t* error, const uint32_t* known, const OwnHeads& own);
 // Direction-optimising BFS levels from device roots (uses slots WS_A..WS_G, WS_COUNTERS, WS_CUB).
 int bfs_levels(gre_graph g, const uint32_t* droots, uint32_t nroots, int32_t* level, gre_stats* st, bool record);
 

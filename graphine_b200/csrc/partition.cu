@@ -1008,6 +1008,8 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
   uint32_t* touched;  // offer slots written since the last clear
   GRE_CHECK(ws_array(s, WS_H, P * W, &touched));
   GRE_CHECK(ws_array(s, WS_J, P * L, &recv));
+  uint32_t* lists;  // per-owner offer lists of a light superstep (send side)
+  GRE_CHECK(ws_array(s, WS_M, P * L, &lists));
   GRE_CHECK(ws_array(s, WS_K, L + 1, &deg));
   GRE_CHECK(ws_array(s, WS_L, L + 1, &prefix));
   uint32_t *tstart, *err;
@@ -1037,6 +1039,17 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
   GRE_CUDA(cudaMemsetAsync(pull_counts, 0, 2 * sizeof(unsigned long long), s->stream));
   GRE_CUDA(cudaMemsetAsync(cand, 0xff, sizeof(uint32_t) * P * L, s->stream));  // then cleared slot by slot
   GRE_CUDA(cudaMemsetAsync(touched, 0, sizeof(uint32_t) * P * W, s->stream));
+  // Known distances of the other ranks' slots: upper bounds that let the relaxations drop offers
+  // that cannot improve, as of the last all-gather of the distances (the pulled heavy passes make
+  // one).  This rank's own heads are relaxed in place (OwnHeads), against its current distances.
+  uint32_t* known = dist_all;
+  GRE_CUDA(cudaMemsetAsync(known, 0xff, sizeof(uint32_t) * P * L, s->stream));
+  OwnHeads own;
+  own.lo = me * L;
+  own.len = L;
+  own.dist = dl;
+  own.pend = pend;
+  own.outdeg = s->outdeg;
   GRE_CUDA(cudaStreamSynchronize(s->stream));
   if (xr / L == me) {
     const uint32_t slot = xr - (uint32_t)(me * L), zero = 0, bit = 1u << (slot & 31u);
@@ -1057,8 +1070,7 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
   // offers of this rank's frontier `list` (or bitmap `front`, binned form) over the light or heavy
   // ranges, exchanged with the owners, who keep the smallest and mark improved slots pending
   // `cap` > 0: every rank's offers of this pass are at most cap, and they travel as per-owner
-  // (slot, distance) lists of cap pairs (in the gather buffer, unused by light supersteps) instead
-  // of the dense P * L offer arrays
+  // (slot, distance) lists of cap pairs instead of the dense P * L offer arrays
   auto offer_pass = [&](const uint32_t* list, uint64_t nlist, const uint32_t* front, uint64_t arcs, bool heavy,
                         uint64_t cap) -> int {
     if (nlist && arcs && bdiv && nlist >= L / bdiv) {
@@ -1069,18 +1081,20 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
         k_queue_to_bits<<<grid_for(nlist, 256), 256, 0, s->stream>>>(list, nlist, bits);
         bytes += 4 * W + 4 * nlist;
       }
-      GRE_CHECK(sssp_relax_binned_offer(s->stream, B, bits, off, lend, heavy, col, w, dl, cand, touched, nullptr));
+      GRE_CHECK(sssp_relax_binned_offer(s->stream, B, bits, off, lend, heavy, col, w, dl, cand, touched, known, own, nullptr));
       bytes += 16 * L + W * 4;  // rows scanned and their frontier bits (arcs below)
     } else if (nlist && arcs) {
       k_part_range_degrees<<<grid_for(nlist, 256), 256, 0, s->stream>>>(list, nlist, off, lend, heavy, deg);
       GRE_CUDA(cub::DeviceScan::ExclusiveSum(cubtmp, cubbytes, deg, prefix, nlist + 1, s->stream));
       GRE_CHECK(sssp_relax_tiles(s->stream, list, nlist, prefix, arcs, tstart, heavy ? lend : off, col, w, dl, cand, touched,
-                                 err));
+                                 err, known, own));
       bytes += 16 * nlist;
     }
-    if (cap) {
+    if (P == 1) {  // every head is this rank's own, relaxed in place: nothing was offered
+      bytes += 12 * arcs;
+    } else if (cap) {
       const uint64_t block = cap + 1;  // uint2: the count, then the pairs
-      uint2* send = (uint2*)dist_all;
+      uint2* send = (uint2*)lists;
       GRE_CUDA(cudaMemset2DAsync(send, 8 * block, 0, 8, P, s->stream));
       const dim3 grid((unsigned)std::min<uint64_t>(grid_for(W, 256), 4 * 148), (unsigned)P);
       k_part_offers_pack<<<grid, 256, 0, s->stream>>>(W, touched, cand, send, block, cap, err);

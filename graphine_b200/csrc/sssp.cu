@@ -113,6 +113,32 @@ __global__ void k_tile_starts(const uint64_t* __restrict__ prefix, uint64_t nq, 
   }
 }
 
+// Offer forms: an arc to head x offering nd.  A head in `own` is relaxed in place (its distance
+// probed, lowered by atomic min, its pending bit set when it has out-arcs); another head is
+// probed against known[x] (when given) and the offer array, and offered by atomic min with its
+// bit in `touched`.  probe() returns the value nd must beat; commit() applies an offer that does.
+struct OfferArc {
+  uint64_t lx;
+  bool mine;
+  __device__ __forceinline__ uint32_t probe(const OwnHeads& o, const uint32_t* known, const uint32_t* offers, uint32_t x,
+                                            uint32_t nd) {
+    lx = (uint64_t)x - o.lo;
+    mine = lx < o.len;
+    if (mine) return __ldcg(o.dist + lx);
+    if (known && nd >= __ldcg(known + x)) return 0u;
+    return __ldcg(offers + x);
+  }
+  __device__ __forceinline__ void commit(const OwnHeads& o, uint32_t* offers, uint32_t* touched, uint32_t x, uint32_t nd) const {
+    if (mine) {
+      atomicMin(o.dist + lx, nd);
+      if (o.outdeg[lx]) atomicOr(o.pend + (lx >> 5), 1u << (lx & 31u));
+    } else {
+      atomicMin(offers + x, nd);
+      if (touched) atomicOr(touched + (x >> 5), 1u << (x & 31u));
+    }
+  }
+};
+
 // OFFER: the owners' distances come from srcdist and `dist` is a separate offer array (the
 // partitioned path); otherwise from dist itself.  Either way an improved entry sets its bit in
 // `changed` when that bitmap is given.
@@ -122,7 +148,8 @@ __global__ void __launch_bounds__(kTileThreads) k_sssp_relax(const uint32_t* __r
                                                              const uint64_t* __restrict__ base, const uint32_t* __restrict__ col,
                                                              const uint32_t* __restrict__ w, const uint32_t* __restrict__ srcdist,
                                                              uint32_t* __restrict__ dist, uint32_t* __restrict__ changed,
-                                                             uint32_t* __restrict__ error) {
+                                                             uint32_t* __restrict__ error, const uint32_t* __restrict__ known,
+                                                             const OwnHeads own) {
   using OwnerScan = cub::BlockScan<uint32_t, kTileThreads>;
   __shared__ uint64_t s_arc[kTile + 1];                // arc index at tile position s_rel[j]
   __shared__ uint32_t s_du[kTile + 1];                 // distance of owner j
@@ -183,18 +210,32 @@ __global__ void __launch_bounds__(kTileThreads) k_sssp_relax(const uint32_t* __r
       v[k] = ok ? __ldg(col + arc) : 0u;
       wt[k] = ok ? __ldg(w + arc) : 0u;
     }
+    if (OFFER) {
+      OfferArc oa[kTileItems];
 #pragma unroll
-    for (int k = 0; k < kTileItems; ++k) {
-      const bool ok = (uint32_t)k * kTileThreads + threadIdx.x < len;
-      dv[k] = ok ? __ldcg(dist + v[k]) : 0u;
-    }
+      for (int k = 0; k < kTileItems; ++k) {
+        const bool ok = (uint32_t)k * kTileThreads + threadIdx.x < len;
+        dv[k] = ok ? oa[k].probe(own, known, dist, v[k], du[k] + wt[k]) : 0u;
+      }
 #pragma unroll
-    for (int k = 0; k < kTileItems; ++k) {
-      const bool ok = (uint32_t)k * kTileThreads + threadIdx.x < len;
-      const uint32_t nd = du[k] + wt[k];
-      if (ok && nd < dv[k]) {
-        atomicMin(dist + v[k], nd);
-        if (changed) atomicOr(changed + (v[k] >> 5), 1u << (v[k] & 31u));
+      for (int k = 0; k < kTileItems; ++k) {
+        const uint32_t nd = du[k] + wt[k];
+        if (nd < dv[k]) oa[k].commit(own, dist, changed, v[k], nd);
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < kTileItems; ++k) {
+        const bool ok = (uint32_t)k * kTileThreads + threadIdx.x < len;
+        dv[k] = ok ? __ldcg(dist + v[k]) : 0u;
+      }
+#pragma unroll
+      for (int k = 0; k < kTileItems; ++k) {
+        const bool ok = (uint32_t)k * kTileThreads + threadIdx.x < len;
+        const uint32_t nd = du[k] + wt[k];
+        if (ok && nd < dv[k]) {
+          atomicMin(dist + v[k], nd);
+          if (changed) atomicOr(changed + (v[k] >> 5), 1u << (v[k] & 31u));
+        }
       }
     }
     __syncthreads();
@@ -218,13 +259,16 @@ struct RelaxRange {
   unsigned long long* __restrict__ arcs;  // arcs relaxed (statistics)
   bool heavy;
   const uint32_t* __restrict__ srcdist;  // OFFER form: the rows' own distances (dist holds offers)
+  const uint32_t* __restrict__ known;    // OFFER form: upper bounds of the heads' distances (may be null)
+  OwnHeads oh;                           // OFFER form: heads relaxed in place
   __device__ __forceinline__ bool in(uint32_t v) const { return (__ldg(front + (v >> 5)) >> (v & 31u)) & 1u; }
   __device__ __forceinline__ void range(uint32_t v, uint64_t* lo, uint64_t* hi) const {
     *lo = heavy ? lend[v] : off[v];
     *hi = heavy ? off[v + 1] : lend[v];
   }
   // arcs a, a + step, ... < hi offered du + w; four column/weight loads, then four distance
-  // probes in flight per lane.  OFFER: dist is a separate offer array and no changed bit is set.
+  // probes in flight per lane.  OFFER: dist is a separate offer array, probed and committed as
+  // OfferArc says.
   template <bool OFFER>
   __device__ __forceinline__ uint32_t own(uint32_t v) const { return __ldcg((OFFER ? srcdist : dist) + v); }
   template <bool OFFER>
@@ -236,19 +280,31 @@ struct RelaxRange {
         x[k] = __ldg(col + a + k * step);
         nd[k] = du + __ldg(w + a + k * step);
       }
+      if (OFFER) {
+        OfferArc oa[4];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) dv[k] = __ldcg(dist + x[k]);
+        for (int k = 0; k < 4; ++k) dv[k] = oa[k].probe(oh, known, dist, x[k], nd[k]);
 #pragma unroll
-      for (int k = 0; k < 4; ++k)
-        if (nd[k] < dv[k]) {
-          atomicMin(dist + x[k], nd[k]);
-          if (changed) atomicOr(changed + (x[k] >> 5), 1u << (x[k] & 31u));
-        }
+        for (int k = 0; k < 4; ++k)
+          if (nd[k] < dv[k]) oa[k].commit(oh, dist, changed, x[k], nd[k]);
+      } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) dv[k] = __ldcg(dist + x[k]);
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          if (nd[k] < dv[k]) {
+            atomicMin(dist + x[k], nd[k]);
+            if (changed) atomicOr(changed + (x[k] >> 5), 1u << (x[k] & 31u));
+          }
+      }
     }
     for (; a < hi; a += step) {
       const uint32_t x = __ldg(col + a);
       const uint32_t nd = du + __ldg(w + a);
-      if (nd < __ldcg(dist + x)) {
+      if (OFFER) {
+        OfferArc oa;
+        if (nd < oa.probe(oh, known, dist, x, nd)) oa.commit(oh, dist, changed, x, nd);
+      } else if (nd < __ldcg(dist + x)) {
         atomicMin(dist + x, nd);
         if (changed) atomicOr(changed + (x >> 5), 1u << (x & 31u));
       }
@@ -527,8 +583,9 @@ __global__ void k_sssp_classes(uint64_t n, const uint64_t* __restrict__ off, con
 
 int sssp_relax_binned_offer(cudaStream_t stream, const DegreeBins& B, const uint32_t* front, const uint64_t* off,
                             const uint64_t* lend, bool heavy, const uint32_t* col, const uint32_t* w, const uint32_t* srcdist,
-                            uint32_t* offers, uint32_t* touched, unsigned long long* arcs) {
-  RelaxRange R{front, off, lend, col, w, offers, touched, arcs, heavy, srcdist};
+                            uint32_t* offers, uint32_t* touched, const uint32_t* known, const OwnHeads& own,
+                            unsigned long long* arcs) {
+  RelaxRange R{front, off, lend, col, w, offers, touched, arcs, heavy, srcdist, known, own};
   return relax_binned<true>(B, R, stream);
 }
 
@@ -744,7 +801,7 @@ bool sssp_pull_enabled() { return pull_enabled(); }
 // The relaxation of one frontier pass: tile starts, then k_sssp_relax over one wave of CTAs.
 int sssp_relax_tiles(cudaStream_t stream, const uint32_t* queue, uint64_t nq, const uint64_t* prefix, uint64_t total,
                      uint32_t* tstart, const uint64_t* base, const uint32_t* col, const uint32_t* w, const uint32_t* srcdist,
-                     uint32_t* dist, uint32_t* changed, uint32_t* error) {
+                     uint32_t* dist, uint32_t* changed, uint32_t* error, const uint32_t* known, const OwnHeads& own) {
   if (!total) return GRE_SUCCESS;
   const uint64_t ntiles = (total + kTile - 1) / kTile;
   k_tile_starts<<<grid_for(nq, 256), 256, 0, stream>>>(prefix, nq, tstart);
@@ -754,10 +811,10 @@ int sssp_relax_tiles(cudaStream_t stream, const uint32_t* queue, uint64_t nq, co
   const int grid = (int)std::min<uint64_t>(ntiles, (uint64_t)num_sms() * (offer ? relax_blocks_per_sm<true>() : relax_blocks_per_sm<false>()));
   if (!offer)
     k_sssp_relax<false><<<grid, kTileThreads, 0, stream>>>(queue, nq, prefix, total, tstart, base, col, w, nullptr, dist, changed,
-                                                           error);
+                                                           error, nullptr, OwnHeads());
   else
     k_sssp_relax<true><<<grid, kTileThreads, 0, stream>>>(queue, nq, prefix, total, tstart, base, col, w, srcdist, dist, changed,
-                                                          error);
+                                                          error, known, own);
   GRE_LAUNCH_CHECK();
   return GRE_SUCCESS;
 }
@@ -896,7 +953,7 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
     GRE_CHECK(init_counters(g, cnt, 0, (uint32_t)nfar, (uint32_t)nb));
     if (total) {
       GRE_CHECK(sssp_relax_tiles(g->stream, list, nlist, prefix, total, tstart, heavy ? lend : off, col, w, dist, dist, changed,
-                                 cnt + 1));
+                                 cnt + 1, nullptr, OwnHeads()));
       k_sssp_classify<<<grid_for(nwords, 256, 4), 256, 0, g->stream>>>(nwords, changed, dist, lbits, hbits, limit, out_near, infar,
                                                                         far, inbucket, blist, cnt);
     }
