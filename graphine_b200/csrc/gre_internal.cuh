@@ -385,6 +385,9 @@ int sssp_split_rows(cudaStream_t stream, uint64_t rows, const uint64_t* off, con
 // whether heavy passes may pull (GRE_SSSP_BINNED, GRE_SSSP_PULL).
 uint64_t sssp_binned_divisor();
 bool sssp_pull_enabled();
+// A heavy pass with at least m / sssp_pull_arcs_divisor() arcs pulls whatever its member count
+// (GRE_SSSP_PULL_ARCS; 0: never by arcs).
+uint64_t sssp_pull_arcs_divisor();
 int sssp_relax_tiles(cudaStream_t stream, const uint32_t* queue, uint64_t nq, const uint64_t* prefix, uint64_t total,
                      uint32_t* tstart, const uint64_t* base, const uint32_t* col, const uint32_t* w, const uint32_t* srcdist,
                      uint32_t* dist, uint32_t* changed, uint32_t* error, const uint32_t* known, const OwnHeads& own);

@@ -330,7 +330,8 @@ struct SsspCounters {
   unsigned long long min_far;     // smallest distance left pending
   unsigned long long arcs;        // light arcs of the frontier
   unsigned long long bucket_new;  // slots that joined the bucket
-  unsigned long long pad[3];
+  unsigned long long heavy_new;   // their heavy arcs
+  unsigned long long pad[2];
 };
 
 __global__ void __launch_bounds__(256) k_part_sssp_select(uint64_t W, uint32_t* __restrict__ pend, const uint32_t* __restrict__ dist, uint32_t limit,
@@ -339,7 +340,7 @@ __global__ void __launch_bounds__(256) k_part_sssp_select(uint64_t W, uint32_t* 
   __shared__ uint32_t stage[8][1024];
   WarpLists<1, 1024> out(stage[threadIdx.x >> 5]);
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  unsigned long long left = 0, arcs = 0, joined = 0;
+  unsigned long long left = 0, arcs = 0, joined = 0, heavy = 0;
   uint32_t dmin = 0xffffffffu;
   for (uint64_t base = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) & ~31ull; base < W; base += stride) {
     const uint64_t w = base + (threadIdx.x & 31u);
@@ -357,7 +358,10 @@ __global__ void __launch_bounds__(256) k_part_sssp_select(uint64_t W, uint32_t* 
           const uint64_t a0 = off[i], am = lend[i], a1 = off[i + 1];
           take = am > a0;
           arcs += am - a0;
-          if (a1 > am && !((inw >> b) & 1u)) join |= 1u << b;
+          if (a1 > am && !((inw >> b) & 1u)) {
+            join |= 1u << b;
+            heavy += a1 - am;
+          }
         } else {
           keep |= 1u << b;
           ++left;
@@ -378,11 +382,13 @@ __global__ void __launch_bounds__(256) k_part_sssp_select(uint64_t W, uint32_t* 
     left += __shfl_xor_sync(0xffffffffu, left, o);
     arcs += __shfl_xor_sync(0xffffffffu, arcs, o);
     joined += __shfl_xor_sync(0xffffffffu, joined, o);
+    heavy += __shfl_xor_sync(0xffffffffu, heavy, o);
   }
   if ((threadIdx.x & 31u) == 0) {
     if (left) atomicAdd(&c->pending, left);
     if (arcs) atomicAdd(&c->arcs, arcs);
     if (joined) atomicAdd(&c->bucket_new, joined);
+    if (heavy) atomicAdd(&c->heavy_new, heavy);
     if (dmin != 0xffffffffu) atomicMin(&c->min_far, (unsigned long long)dmin);
   }
 }
@@ -1028,6 +1034,7 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
   const uint64_t bdiv = sssp_binned_divisor();
   const bool pull = p->w_sym && delta && sssp_pull_enabled();
   const uint64_t sparse = part_sparse_offers();
+  const uint64_t pdiv = sssp_pull_arcs_divisor();
 
   RunTimer timer(s);
   uint32_t xr = 0;
@@ -1064,7 +1071,7 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
   // distance + delta.
   const uint32_t width = delta ? delta : 0xffffffffu;
   uint32_t limit = width;
-  uint64_t relaxed = 0, bytes = 0, bucket = 0;
+  uint64_t relaxed = 0, bytes = 0, bucket = 0, bucket_heavy = 0;
   uint32_t steps = 0;
   std::vector<SsspCounters> h(P);
   // offers of this rank's frontier `list` (or bitmap `front`, binned form) over the light or heavy
@@ -1114,7 +1121,7 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
     return GRE_SUCCESS;
   };
   for (;;) {
-    const SsspCounters zero{0, 0, 0xffffffffffffffffull, 0, 0, {0, 0, 0}};
+    const SsspCounters zero{0, 0, 0xffffffffffffffffull, 0, 0, 0, {0, 0}};
     GRE_CUDA(cudaMemcpyAsync(c, &zero, sizeof zero, cudaMemcpyHostToDevice, s->stream));
     k_part_sssp_select<<<grid_for(W, 256), 256, 0, s->stream>>>(W, pend, dl, limit, off, lend, inb, queue, c);
     GRE_LAUNCH_CHECK();
@@ -1126,6 +1133,7 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
       near += x.near;
       pending += x.pending;
       bucket += x.bucket_new;
+      bucket_heavy += x.heavy_new;
       min_far = std::min<uint64_t>(min_far, x.min_far);
     }
     bytes += 4 * W + 8 * (h[me].near + h[me].pending);
@@ -1139,7 +1147,8 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
       continue;
     }
     if (bucket) {  // the bucket is settled: its heavy arcs, once (every rank sees the same sums)
-      if (pull && bdiv && bucket >= P * L / bdiv) {
+      // pulled when the bucket has many members or many heavy arcs (the same sums on every rank)
+      if (pull && bdiv && (bucket >= P * L / bdiv || (pdiv && bucket_heavy * pdiv >= p->m))) {
         GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLGATHER, dl, dist_all, 4 * L));
         GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLGATHER, inb, inb_all, 4 * W));
         GRE_CHECK(sssp_pull_binned(s->stream, B, inb_all, off, lend, true, col, w, dist_all, dl, pend, limit, pull_counts));
@@ -1166,6 +1175,7 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
       }
       GRE_CUDA(cudaMemsetAsync(inb, 0, sizeof(uint32_t) * W, s->stream));
       bucket = 0;
+      bucket_heavy = 0;
       ++steps;
       stats_record(st, 0);
       continue;

@@ -5,7 +5,7 @@
 // the result is bit-exact whatever the relaxation order.  Differences from the reference's
 // superstep, chosen for the GPU:
 //   * near-far ordering (Davidson et al., IPDPS 2014): improved vertices below a moving limit
-//     form the next frontier, the others wait in a far pile until the limit (raised by a bucket
+//     form the next frontier, the others wait in a far set until the limit (raised by a bucket
 //     width delta, or to the smallest waiting distance + delta) passes them; with the light/heavy
 //     split of delta-stepping (Meyer and Sanders 2003) only arcs lighter than delta are relaxed
 //     inside a bucket and a settled bucket's heavy arcs once.  On RMAT this relaxes each arc
@@ -15,7 +15,10 @@
 //     serialise a warp;
 //   * an improvement is a fire-and-forget atomic min on the distance plus a bit in a changed
 //     bitmap: no thread waits for an atomic's reply (hub heads receive thousands per superstep),
-//     and a pass over the bitmap builds the next frontier and far pile without duplicates;
+//     and a pass over the bitmap builds the next frontier and far set without duplicates;
+//   * the far set is a bitmap: a limit rise scans it, reading the far vertices' distances in
+//     vertex order, 32 to a word (against a list of far vertices, read at random: RMAT-26 SSSP
+//     18.5 -> 17.8 ms);
 //   * the distance of a frontier vertex is read when its tile starts (not a copy taken at the
 //     start of the superstep), which can only lower the values sent;
 //   * vertices without out-arcs are never queued (they have nothing to relax).
@@ -603,18 +606,20 @@ int sssp_split_rows(cudaStream_t stream, uint64_t rows, const uint64_t* off, con
   return GRE_SUCCESS;
 }
 
-// Changed vertices -> next queues, one lane per bitmap word (the word is cleared).  Below the
-// limit a vertex joins the near queue if it has light arcs, and the bucket list (once per
-// bucket) if it has heavy arcs; its far entry, if any, becomes void.  At or above the limit it
-// joins the far pile unless already there.  Vertices without out-arcs are dropped.
-constexpr int kStage = 512;  // items per list that a warp stages in shared memory (3 lists x 8 warps: 48 KB)
+constexpr int kStage = 512;  // items per list that a warp stages in shared memory (2 lists x 8 warps: 32 KB)
 
+// Classify the vertices improved by a pass (bits of `changed`, one lane per word, cleared here):
+// below the limit a vertex with light arcs joins the near queue and one with heavy arcs the
+// bucket list (once: `inbucket`), and leaves the far set; at or above the limit it joins the far
+// set (a bitmap, `infar`).  Vertices without out-arcs are dropped.  counters[0] and [4] are the
+// queue and list lengths, counters[2] the far set's size.
 __global__ void __launch_bounds__(256) k_sssp_classify(uint64_t nwords, uint32_t* __restrict__ changed, const uint32_t* __restrict__ dist,
                                 const uint32_t* __restrict__ lbits, const uint32_t* __restrict__ hbits, uint32_t near_limit,
-                                uint32_t* __restrict__ near, uint32_t* __restrict__ infar, uint32_t* __restrict__ far,
+                                uint32_t* __restrict__ near, uint32_t* __restrict__ infar,
                                 uint32_t* __restrict__ inbucket, uint32_t* __restrict__ blist, uint32_t* __restrict__ counters) {
-  __shared__ uint32_t stage[8][3 * kStage];
-  WarpLists<3, kStage> out(stage[threadIdx.x >> 5]);
+  __shared__ uint32_t stage[8][2 * kStage];
+  WarpLists<2, kStage> out(stage[threadIdx.x >> 5]);
+  int far_delta = 0;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t base = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) & ~31ull; base < nwords; base += stride) {
     const uint64_t wi = base + (threadIdx.x & 31u);
@@ -631,7 +636,7 @@ __global__ void __launch_bounds__(256) k_sssp_classify(uint64_t nwords, uint32_t
     }
     uint32_t set_far = 0, clear_far = 0, set_bucket = 0;
     while (__any_sync(0xffffffffu, bits != 0)) {
-      bool to_near = false, to_far = false, to_bucket = false;
+      bool to_near = false, to_bucket = false;
       uint32_t v = 0;
       if (bits) {
         const uint32_t b = __ffs(bits) - 1;
@@ -647,21 +652,21 @@ __global__ void __launch_bounds__(256) k_sssp_classify(uint64_t nwords, uint32_t
             }
             if (fbits & (1u << b)) clear_far |= 1u << b;
           } else if (!(fbits & (1u << b))) {
-            to_far = true;
             set_far |= 1u << b;
           }
         }
       }
       out.push<0>(to_near, v, counters, near);
-      out.push<1>(to_far, v, counters + 2, far);
-      out.push<2>(to_bucket, v, counters + 4, blist);
+      out.push<1>(to_bucket, v, counters + 4, blist);
     }
     if (set_far | clear_far) infar[wi] = (fbits | set_far) & ~clear_far;  // one lane owns the word
     if (set_bucket) inbucket[wi] = bbits | set_bucket;
+    far_delta += __popc(set_far) - __popc(clear_far);
   }
   out.flush<0>(counters, near);
-  out.flush<1>(counters + 2, far);
-  out.flush<2>(counters + 4, blist);
+  out.flush<1>(counters + 4, blist);
+  far_delta = __reduce_add_sync(0xffffffffu, far_delta);
+  if ((threadIdx.x & 31u) == 0 && far_delta) atomicAdd(counters + 2, (uint32_t)far_delta);
 }
 
 // The bucket's heavy arcs have been relaxed: its members leave the bucket list.
@@ -685,46 +690,64 @@ __global__ void k_sssp_seed(uint32_t src, const uint64_t* __restrict__ off, cons
   }
 }
 
-// Near-far pile split: far vertices whose distance is now below the limit move to the near
-// queue and the bucket list (as in k_sssp_classify; their far bit is cleared), the others stay;
-// entries whose far bit was cleared (the vertex went to the near queue since) are dropped.
-// counters[3] gets the smallest distance left.
-__global__ void __launch_bounds__(256) k_far_split(const uint32_t* __restrict__ far, uint64_t nfar, const uint32_t* __restrict__ dist, uint32_t near_limit,
-                            const uint32_t* __restrict__ lbits, const uint32_t* __restrict__ hbits, uint32_t* __restrict__ infar,
-                            uint32_t* __restrict__ near, uint32_t* __restrict__ far_out, uint32_t* __restrict__ inbucket,
-                            uint32_t* __restrict__ blist, uint32_t* __restrict__ counters) {
-  __shared__ uint32_t stage[8][3 * kStage];
-  WarpLists<3, kStage> out(stage[threadIdx.x >> 5]);
+// Near-far split when the limit rises: every vertex of the far set (bitmap `infar`) whose
+// distance is now below the limit leaves it for the near queue (light arcs) and the bucket list
+// (heavy arcs; once: `inbucket`), as in k_sssp_classify; the others stay.  counters[2] (the far
+// set's size) drops by the vertices that left, counters[3] gets the smallest distance left.  A
+// scan of the bitmap reads the distances of far vertices in vertex order, 32 to a word.
+__global__ void __launch_bounds__(256) k_far_split(uint64_t nwords, uint32_t* __restrict__ infar, const uint32_t* __restrict__ dist,
+                                                   uint32_t near_limit, const uint32_t* __restrict__ lbits,
+                                                   const uint32_t* __restrict__ hbits, uint32_t* __restrict__ near,
+                                                   uint32_t* __restrict__ inbucket, uint32_t* __restrict__ blist,
+                                                   uint32_t* __restrict__ counters) {
+  __shared__ uint32_t stage[8][2 * kStage];
+  WarpLists<2, kStage> out(stage[threadIdx.x >> 5]);
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  uint32_t dmin = 0xffffffffu;
-  for (uint64_t base = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) & ~31ull; base < nfar; base += stride) {
-    const uint64_t i = base + (threadIdx.x & 31u);
-    bool to_near = false, keep = false, to_bucket = false;
-    uint32_t v = 0;
-    if (i < nfar) {
-      v = far[i];
-      const uint32_t bit = 1u << (v & 31u);
-      if (infar[v >> 5] & bit) {
+  uint32_t dmin = 0xffffffffu, left = 0;
+  for (uint64_t base = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) & ~31ull; base < nwords; base += stride) {
+    const uint64_t wi = base + (threadIdx.x & 31u);
+    uint32_t bits = wi < nwords ? infar[wi] : 0u;
+    const uint32_t fbits = bits;
+    uint32_t moved = 0, set_bucket = 0, bbits = 0, lw = 0, hw = 0;
+    if (bits) {
+      bbits = inbucket[wi];
+      lw = lbits[wi];
+      hw = hbits[wi];
+    }
+    while (__any_sync(0xffffffffu, bits != 0)) {
+      bool to_near = false, to_bucket = false;
+      uint32_t v = 0;
+      if (bits) {
+        const uint32_t b = __ffs(bits) - 1;
+        bits &= bits - 1;
+        v = (uint32_t)(wi << 5) + b;
         const uint32_t d = dist[v];
         if (d < near_limit) {
-          atomicAnd(infar + (v >> 5), ~bit);
-          to_near = (lbits[v >> 5] & bit) != 0;
-          if (hbits[v >> 5] & bit) to_bucket = !(atomicOr(inbucket + (v >> 5), bit) & bit);
+          moved |= 1u << b;
+          to_near = (lw >> b) & 1u;
+          if (((hw >> b) & 1u) && !(bbits & (1u << b))) {
+            to_bucket = true;
+            set_bucket |= 1u << b;
+          }
         } else {
-          keep = true;
           dmin = min(dmin, d);
         }
       }
+      out.push<0>(to_near, v, counters, near);
+      out.push<1>(to_bucket, v, counters + 4, blist);
     }
-    out.push<0>(to_near, v, counters, near);
-    out.push<1>(keep, v, counters + 2, far_out);
-    out.push<2>(to_bucket, v, counters + 4, blist);
+    if (moved) infar[wi] = fbits & ~moved;
+    if (set_bucket) inbucket[wi] = bbits | set_bucket;
+    left += __popc(moved);
   }
   out.flush<0>(counters, near);
-  out.flush<1>(counters + 2, far_out);
-  out.flush<2>(counters + 4, blist);
+  out.flush<1>(counters + 4, blist);
   dmin = __reduce_min_sync(0xffffffffu, dmin);
-  if ((threadIdx.x & 31u) == 0 && dmin != 0xffffffffu) atomicMin(counters + 3, dmin);
+  left = __reduce_add_sync(0xffffffffu, left);
+  if ((threadIdx.x & 31u) == 0) {
+    if (dmin != 0xffffffffu) atomicMin(counters + 3, dmin);
+    if (left) atomicSub(counters + 2, left);
+  }
 }
 
 struct AddU64 {
@@ -758,8 +781,8 @@ int sssp_delta(gre_graph g, uint32_t* delta) {
   return GRE_SUCCESS;
 }
 
-// counters: [0] near appends, [1] overflow flag, [2] far appends (from the current far pile
-// size), [3] smallest far distance left by a split, [4] bucket-list appends (from its size)
+// counters: [0] near appends, [1] overflow flag, [2] size of the far set, [3] smallest far
+// distance left by a split, [4] bucket-list appends (from its size)
 static int init_counters(gre_graph g, uint32_t* cnt, uint32_t near, uint32_t nfar, uint32_t nbucket) {
   const uint32_t h[8] = {near, 0, nfar, 0xffffffffu, nbucket, 0, 0, 0};  // pageable: staged before the call returns
   GRE_CUDA(cudaMemcpyAsync(cnt, h, sizeof h, cudaMemcpyHostToDevice, g->stream));
@@ -797,6 +820,15 @@ static bool pull_enabled() {
   return true;
 }
 bool sssp_pull_enabled() { return pull_enabled(); }
+
+// A heavy pass whose bucket has at least m / d heavy arcs pulls even when the bucket has fewer
+// than n / sssp_binned_divisor() members (a few hubs can carry a large share of the arcs): d from
+// GRE_SSSP_PULL_ARCS, default 16; 0 decides by the member count alone.
+static uint64_t pull_arcs_divisor() {
+  if (const char* e = getenv("GRE_SSSP_PULL_ARCS")) return strtoull(e, nullptr, 10);
+  return 16;
+}
+uint64_t sssp_pull_arcs_divisor() { return pull_arcs_divisor(); }
 
 // The relaxation of one frontier pass: tile starts, then k_sssp_relax over one wave of CTAs.
 int sssp_relax_tiles(cudaStream_t stream, const uint32_t* queue, uint64_t nq, const uint64_t* prefix, uint64_t total,
@@ -851,13 +883,11 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
   const uint64_t* lend = delta ? g->sssp_split.lsplit : g->off + 1;  // end of each row's light arcs
   const uint32_t* col = delta ? g->sssp_split.col : g->col;
   const uint32_t* w = delta ? g->sssp_split.w : g->w32;
-  uint32_t *qa, *qb, *changed, *cnt, *fa, *fb, *infar, *tstart, *inbucket, *blist;
+  uint32_t *qa, *qb, *changed, *cnt, *infar, *tstart, *inbucket, *blist;
   uint64_t *deg, *prefix;
   GRE_CHECK(ws_array(g, WS_A, n, &qa));
   GRE_CHECK(ws_array(g, WS_B, n, &qb));
   GRE_CHECK(ws_array(g, WS_C, nwords, &changed));
-  GRE_CHECK(ws_array(g, WS_D, n, &fa));
-  GRE_CHECK(ws_array(g, WS_E, n, &fb));
   GRE_CHECK(ws_array(g, WS_F, n + 1, &deg));
   GRE_CHECK(ws_array(g, WS_G, n + 1, &prefix));
   GRE_CHECK(ws_array(g, WS_I, g->m / kTile + 2, &tstart));
@@ -877,6 +907,7 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
   GRE_CHECK(ensure_bins(g, sym));
   const DegreeBins& bins = sym ? g->bins_in : g->bins_out;
   const uint64_t bdiv = binned_frontier();
+  const uint64_t pdiv = pull_arcs_divisor();
   size_t cubbytes = 0;
   void* cubtmp = nullptr;
   cub::DeviceScan::ExclusiveSum(nullptr, cubbytes, deg, prefix, n + 1, g->stream);
@@ -891,8 +922,6 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
   uint64_t nq = 0, nfar = 0, nb = 0, relaxed = 0, bytes = 0;
   uint32_t* q = qa;
   uint32_t* nqueue = qb;
-  uint32_t* far = fa;
-  uint32_t* far2 = fb;
   uint32_t steps = 0;
   uint32_t h[8];
   auto read_counters = [&]() -> int {
@@ -911,9 +940,20 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
   nq = h[0];
   nb = h[4];
   // one relaxation pass over `list` (light or heavy ranges), the improvements classified into
-  // the next near queue, the bucket list and the far pile
+  // the next near queue, the bucket list and the far set
   auto pass = [&](const uint32_t* list, uint64_t nlist, bool heavy, uint32_t* out_near) -> int {
-    if (bdiv && nlist >= n / bdiv && nlist > 0) {
+    bool bins_form = bdiv && nlist >= n / bdiv && nlist > 0;
+    uint64_t total = 0;
+    if (!bins_form) {  // the arcs of the frontier, for the tiles
+      if (heavy) k_sssp_degrees<true><<<grid_for(nlist, 256), 256, 0, g->stream>>>(list, nlist, off, lend, deg);
+      else k_sssp_degrees<false><<<grid_for(nlist, 256), 256, 0, g->stream>>>(list, nlist, off, lend, deg);
+      GRE_CUDA(cub::DeviceScan::ExclusiveSum(cubtmp, cubbytes, deg, prefix, nlist + 1, g->stream));
+      GRE_CUDA(cudaMemcpyAsync(&total, prefix + nlist, sizeof total, cudaMemcpyDeviceToHost, g->stream));
+      GRE_CUDA(cudaStreamSynchronize(g->stream));
+      // a small bucket with many heavy arcs (hubs among its members) pulls them instead
+      if (heavy && pull && bdiv && pdiv && total && total * pdiv >= g->m) bins_form = true;
+    }
+    if (bins_form) {
       // the heavy pass's frontier is the bucket, already a bitmap; a light frontier is made one
       // in the scan buffer (free in this form of the pass)
       uint32_t* front = inbucket;
@@ -935,7 +975,7 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
         GRE_CHECK(relax_binned<false>(bins, R, g->stream));
       }
       k_sssp_classify<<<grid_for(nwords, 256, 4), 256, 0, g->stream>>>(nwords, changed, dist, lbits, hbits, limit, out_near, infar,
-                                                                        far, inbucket, blist, cnt);
+                                                                        inbucket, blist, cnt);
       GRE_LAUNCH_CHECK();
       GRE_CHECK(read_counters());
       bytes += 4 * n + n / 8 + 8 * (uint64_t)(h[0] + h[2] - nfar + h[4] - nb);  // rows scanned, bitmap (arcs below)
@@ -944,18 +984,12 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
       ++steps;
       return GRE_SUCCESS;
     }
-    if (heavy) k_sssp_degrees<true><<<grid_for(nlist, 256), 256, 0, g->stream>>>(list, nlist, off, lend, deg);
-    else k_sssp_degrees<false><<<grid_for(nlist, 256), 256, 0, g->stream>>>(list, nlist, off, lend, deg);
-    GRE_CUDA(cub::DeviceScan::ExclusiveSum(cubtmp, cubbytes, deg, prefix, nlist + 1, g->stream));
-    uint64_t total = 0;
-    GRE_CUDA(cudaMemcpyAsync(&total, prefix + nlist, sizeof total, cudaMemcpyDeviceToHost, g->stream));
-    GRE_CUDA(cudaStreamSynchronize(g->stream));
     GRE_CHECK(init_counters(g, cnt, 0, (uint32_t)nfar, (uint32_t)nb));
     if (total) {
       GRE_CHECK(sssp_relax_tiles(g->stream, list, nlist, prefix, total, tstart, heavy ? lend : off, col, w, dist, dist, changed,
                                  cnt + 1, nullptr, OwnHeads()));
       k_sssp_classify<<<grid_for(nwords, 256, 4), 256, 0, g->stream>>>(nwords, changed, dist, lbits, hbits, limit, out_near, infar,
-                                                                        far, inbucket, blist, cnt);
+                                                                        inbucket, blist, cnt);
     }
     GRE_LAUNCH_CHECK();
     GRE_CHECK(read_counters());
@@ -1000,17 +1034,16 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
       }
       if (p == 0) limit = limit > 0xffffffffu - delta ? 0xffffffffu : limit + delta;
       else limit = lowest > 0xffffffffu - delta ? 0xffffffffu : lowest + delta;
-      GRE_CHECK(init_counters(g, cnt, 0, 0, 0));
-      k_far_split<<<grid_for(nfar, 256, 4), 256, 0, g->stream>>>(far, nfar, dist, limit, lbits, hbits, infar, q, far2, inbucket,
-                                                                  blist, cnt);
+      GRE_CHECK(init_counters(g, cnt, 0, (uint32_t)nfar, 0));
+      k_far_split<<<grid_for(nwords, 256, 4), 256, 0, g->stream>>>(nwords, infar, dist, limit, lbits, hbits, q, inbucket, blist,
+                                                                    cnt);
       GRE_LAUNCH_CHECK();
       GRE_CHECK(read_counters());
-      bytes += 8 * nfar + 4 * (uint64_t)(h[0] + h[2] + h[4]);
+      bytes += 4 * nwords + 4 * nfar + 4 * (uint64_t)(h[0] + h[4]);
       nq = h[0];
       nfar = h[2];
       nb = h[4];
       lowest = h[3];
-      std::swap(far, far2);
     }
   }
   unsigned long long bc[3] = {0, 0, 0};

@@ -521,13 +521,16 @@ def test_s20_cc_properties(rmat20):
     np.testing.assert_array_equal(lab, lab2)
 
 
+@pytest.mark.parametrize("pull_arcs", ["0", "16", "4294967296"], ids=["by-members", "by-arcs", "heavy-always"])
 @pytest.mark.parametrize("pull", ["0", "1"], ids=["push", "pull"])
 @pytest.mark.parametrize("binned", ["0", "4294967296", "64"], ids=["tiles", "bins", "default"])
-def test_sssp_relaxation_forms_agree(monkeypatch, binned, pull):
+def test_sssp_relaxation_forms_agree(monkeypatch, binned, pull, pull_arcs):
     """Arc tiles only, degree bins only (every pass, pushed along the frontier's arcs or pulled
-    by the vertices that can improve), and the default mix give the oracle's distances."""
+    by the vertices that can improve), and the default mix give the oracle's distances; heavy
+    passes pull by the bucket's member count only, also by its heavy arcs, or (almost) always."""
     monkeypatch.setenv("GRE_SSSP_BINNED", binned)
     monkeypatch.setenv("GRE_SSSP_PULL", pull)
+    monkeypatch.setenv("GRE_SSSP_PULL_ARCS", pull_arcs)
     for sym in (True, False):
         n, off, col = G.rmat_host(12, 16, 9, sym)
         g = G.Graph.from_csr(n, off, col, dir=G.InOut if sym else G.Out, symmetric=sym, reorder=True)

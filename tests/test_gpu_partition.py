@@ -117,6 +117,22 @@ def test_partitioned_sssp_forms(monkeypatch, P, binned, pull, sparse):
             np.testing.assert_array_equal(dist, ref[i])
 
 
+@pytest.mark.parametrize("pull_arcs", ["0", "4294967296"], ids=["by-members", "heavy-always"])
+@pytest.mark.parametrize("P", [1, 3])
+def test_partitioned_sssp_heavy_pull_by_arcs(monkeypatch, P, pull_arcs):
+    """Heavy passes pulled by the bucket's member count only, or whenever it has any heavy arcs
+    (the decision from the all-gathered sums, the same on every rank)."""
+    monkeypatch.setenv("GRE_SSSP_PULL_ARCS", pull_arcs)
+    n, off, col, g = _graph(11, True, True)
+    g.set_weights_hash(WSEED)
+    R = O.Restatement.from_csr(n, off, col)
+    roots = G.sample_sources(off, 2, 8)
+    ref = R.sssp_many(roots, WSEED)
+    for i, s in enumerate(roots):
+        for dist, _ in PT.run_local(g, P, lambda part, x: part.sssp(int(s), x)):
+            np.testing.assert_array_equal(dist, ref[i])
+
+
 @pytest.mark.parametrize("P", [1, 2, 3, 4])
 @pytest.mark.parametrize("reorder", [False, True], ids=["plain", "relabelled"])
 def test_partitioned_cc_equals_oracle_and_one_gpu(P, reorder):
