@@ -39,7 +39,7 @@ int cuda_status(cudaError_t e, const char* what, const char* file, int line);
 // until the handle is freed, so repeated runs do no allocation.
 // ---------------------------------------------------------------------------------------------
 enum WsSlot {
-  WS_A = 0, WS_B, WS_C, WS_D, WS_E, WS_F, WS_G, WS_H, WS_I, WS_J, WS_K, WS_L, WS_M,
+  WS_A = 0, WS_B, WS_C, WS_D, WS_E, WS_F, WS_G, WS_H, WS_I, WS_J, WS_K, WS_L, WS_M, WS_N,
   WS_COUNTERS,   // small per-run counters (device-side)
   WS_CUB,        // CUB temporary storage
   WS_OUTBUF,     // device staging of results bound for host memory

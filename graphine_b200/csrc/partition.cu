@@ -319,24 +319,29 @@ __global__ void k_part_sssp_claim(uint64_t L, uint64_t P, const uint32_t* __rest
 }
 
 // Near-far selection with the light/heavy split of delta-stepping (Davidson et al., IPDPS 2014;
-// Meyer and Sanders 2003), as the one-GPU path: pending slots below the limit leave the pending
-// set; those with light arcs ([off, lend)) form this superstep's light frontier, those with heavy
-// arcs ([lend, off+1)) join the bucket, whose heavy arcs are relaxed once when no rank has a
-// light frontier left.  The other pending slots stay, and the smallest of their distances is
-// kept (to raise the limit when the bucket is done).  One lane owns each pending word.
+// Meyer and Sanders 2003), as the one-GPU path.  The slots improved since the last selection
+// (bits of `pend`, cleared here) and, right after the limit rose, every slot of the far set
+// (bitmap `farb`) are examined: below the limit a slot leaves the far set; with light arcs
+// ([off, lend)) it joins this superstep's light frontier, with heavy arcs ([lend, off+1)) the
+// bucket, whose heavy arcs are relaxed once when no rank has a light frontier left.  At or above
+// the limit it joins (or stays in) the far set.  `pending` counts the far set; `min_far` is the
+// smallest distance seen going far (exact after a rescan, a lower bound otherwise: the host
+// passes the previous value in).  One lane owns each word.
 struct SsspCounters {
   unsigned long long near;        // light frontier of this superstep
-  unsigned long long pending;     // left pending (at or above the limit)
-  unsigned long long min_far;     // smallest distance left pending
+  unsigned long long pending;     // slots of the far set (at or above the limit)
+  unsigned long long min_far;     // smallest far distance (see above)
   unsigned long long arcs;        // light arcs of the frontier
   unsigned long long bucket_new;  // slots that joined the bucket
   unsigned long long heavy_new;   // their heavy arcs
   unsigned long long pad[2];
 };
 
-__global__ void __launch_bounds__(256) k_part_sssp_select(uint64_t W, uint32_t* __restrict__ pend, const uint32_t* __restrict__ dist, uint32_t limit,
-                                   const uint64_t* __restrict__ off, const uint64_t* __restrict__ lend, uint32_t* __restrict__ inb,
-                                   uint32_t* __restrict__ queue, SsspCounters* __restrict__ c) {
+__global__ void __launch_bounds__(256) k_part_sssp_select(uint64_t W, uint32_t* __restrict__ pend, uint32_t* __restrict__ farb,
+                                                          bool rescan, const uint32_t* __restrict__ dist, uint32_t limit,
+                                                          const uint64_t* __restrict__ off, const uint64_t* __restrict__ lend,
+                                                          uint32_t* __restrict__ inb, uint32_t* __restrict__ queue,
+                                                          SsspCounters* __restrict__ c) {
   __shared__ uint32_t stage[8][1024];
   WarpLists<1, 1024> out(stage[threadIdx.x >> 5]);
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -344,7 +349,8 @@ __global__ void __launch_bounds__(256) k_part_sssp_select(uint64_t W, uint32_t* 
   uint32_t dmin = 0xffffffffu;
   for (uint64_t base = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) & ~31ull; base < W; base += stride) {
     const uint64_t w = base + (threadIdx.x & 31u);
-    uint32_t bits = w < W ? pend[w] : 0u, keep = 0, join = 0;
+    const uint32_t nb = w < W ? pend[w] : 0u, fb = w < W ? farb[w] : 0u;
+    uint32_t bits = rescan ? nb | fb : nb, far_now = fb, join = 0;
     const uint32_t inw = bits ? inb[w] : 0u;
     while (__any_sync(0xffffffffu, bits != 0)) {
       bool take = false;
@@ -355,6 +361,7 @@ __global__ void __launch_bounds__(256) k_part_sssp_select(uint64_t W, uint32_t* 
         i = (uint32_t)(w << 5) + b;
         const uint32_t d = dist[i];
         if (d < limit) {
+          far_now &= ~(1u << b);
           const uint64_t a0 = off[i], am = lend[i], a1 = off[i + 1];
           take = am > a0;
           arcs += am - a0;
@@ -363,14 +370,15 @@ __global__ void __launch_bounds__(256) k_part_sssp_select(uint64_t W, uint32_t* 
             heavy += a1 - am;
           }
         } else {
-          keep |= 1u << b;
-          ++left;
+          far_now |= 1u << b;
           dmin = min(dmin, d);
         }
       }
       out.push<0>(take, i, (uint32_t*)&c->near, queue);
     }
-    if (w < W && pend[w] != keep) pend[w] = keep;
+    if (nb) pend[w] = 0;
+    if (far_now != fb) farb[w] = far_now;
+    left += __popc(far_now);
     if (join) {
       inb[w] = inw | join;
       joined += __popc(join);
@@ -1007,6 +1015,8 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
   GRE_CHECK(ws_array(s, WS_A, L, &dl));
   GRE_CHECK(ws_array(s, WS_B, P * L, &dist_all));
   GRE_CHECK(ws_array(s, WS_C, W, &pend));
+  uint32_t* farb;  // the far set: slots at or above the limit, examined again when it rises
+  GRE_CHECK(ws_array(s, WS_N, W, &farb));
   GRE_CHECK(ws_array(s, WS_D, L, &queue));
   GRE_CHECK(ws_array(s, WS_F, W, &inb));
   GRE_CHECK(ws_array(s, WS_G, P * W, &inb_all));
@@ -1041,6 +1051,7 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
   GRE_CUDA(cudaMemcpyAsync(&xr, p->xof + src, sizeof xr, cudaMemcpyDeviceToHost, s->stream));
   GRE_CUDA(cudaMemsetAsync(dl, 0xff, sizeof(uint32_t) * L, s->stream));
   GRE_CUDA(cudaMemsetAsync(pend, 0, sizeof(uint32_t) * W, s->stream));
+  GRE_CUDA(cudaMemsetAsync(farb, 0, sizeof(uint32_t) * W, s->stream));
   GRE_CUDA(cudaMemsetAsync(inb, 0, sizeof(uint32_t) * W, s->stream));
   GRE_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), s->stream));
   GRE_CUDA(cudaMemsetAsync(pull_counts, 0, 2 * sizeof(unsigned long long), s->stream));
@@ -1120,14 +1131,19 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
     relaxed += arcs;
     return GRE_SUCCESS;
   };
+  bool rescan = false;                 // the limit rose: examine the far set again
+  unsigned long long far_floor = ~0ull;  // this rank's smallest far distance seen so far
   for (;;) {
-    const SsspCounters zero{0, 0, 0xffffffffffffffffull, 0, 0, 0, {0, 0}};
+    // pageable: staged before the call returns
+    const SsspCounters zero{0, 0, rescan ? 0xffffffffffffffffull : far_floor, 0, 0, 0, {0, 0}};
     GRE_CUDA(cudaMemcpyAsync(c, &zero, sizeof zero, cudaMemcpyHostToDevice, s->stream));
-    k_part_sssp_select<<<grid_for(W, 256), 256, 0, s->stream>>>(W, pend, dl, limit, off, lend, inb, queue, c);
+    k_part_sssp_select<<<grid_for(W, 256), 256, 0, s->stream>>>(W, pend, farb, rescan, dl, limit, off, lend, inb, queue, c);
     GRE_LAUNCH_CHECK();
     GRE_CHECK(exchange(p, xchg, ctx, GRE_XCHG_ALLGATHER, c, call, sizeof(SsspCounters)));
     GRE_CUDA(cudaMemcpyAsync(h.data(), call, sizeof(SsspCounters) * P, cudaMemcpyDeviceToHost, s->stream));
     GRE_CUDA(cudaStreamSynchronize(s->stream));
+    rescan = false;
+    far_floor = h[me].min_far;
     uint64_t near = 0, pending = 0, min_far = ~0ull;
     for (const SsspCounters& x : h) {
       near += x.near;
@@ -1136,7 +1152,7 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
       bucket_heavy += x.heavy_new;
       min_far = std::min<uint64_t>(min_far, x.min_far);
     }
-    bytes += 4 * W + 8 * (h[me].near + h[me].pending);
+    bytes += 12 * W + 8 * h[me].near;  // pending, far and bucket words; the frontier's distances
     if (near) {  // a light superstep
       uint64_t most = 0;  // the most offers any rank can make (the same on every rank)
       for (const SsspCounters& x : h) most = std::max<uint64_t>(most, x.arcs);
@@ -1181,8 +1197,11 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
       continue;
     }
     if (pending == 0) break;
-    // every rank sees the same sums: the same new limit
+    // every rank sees the same sums: the same new limit.  min_far is exact after a rescan and a
+    // lower bound otherwise (a far slot that later left the set may have set it): a rescan that
+    // brings nothing below the new limit computes the exact value for the next rise.
     limit = min_far > 0xffffffffull - width ? 0xffffffffu : (uint32_t)(min_far + width);
+    rescan = true;
   }
   GRE_CUDA(cudaMemsetAsync(bc, 0, sizeof(BfsCounters), s->stream));
   k_part_reached_dist<<<grid_for(L, 256), 256, 0, s->stream>>>(L, dl, s->outdeg, &bc->next_arcs);
