@@ -16,7 +16,7 @@ device-resident outputs; `e2e` runs the same calls with pinned host outputs, the
 copies inside the timed region.  After the timed steps, `batched_vs_plain` reports the batched
 forms against their looped plain forms at equal results (256-source BC, 64-source BFS, 128
 personalised PageRank vectors, a batch of 32 uneven graphs; scale 20) and the PageRank adjoint
-against its forward, plus one 64-source BC batch on the scale-26 graph.  `partitioned` times the
+against its forward, plus 1024-source sampled BC in 16 batches of 64 on the scale-26 graph.  `partitioned` times the
 1D-partitioned BFS, PageRank, SSSP and CC (gre_part_*, graphine_b200/partition.py) over the
 ranks, NCCL exchanges; at one GPU a one-rank communicator, checked equal to the one-GPU calls.
 
@@ -56,7 +56,7 @@ METRIC = "GTEPS & HBM GB/s at RMAT-26 on 1 B200; batched/adjoint vs plain at equ
 SEED = 26
 WSEED = 20240601
 PR_ITERS = 20
-BC_SOURCES = 64
+BC_SOURCES = 1024  # sampled BC sources per rank at the main scale (64 per frontier word)
 REF_SCALE = 18  # scale of the reference arm's bounded sample
 
 
