@@ -383,6 +383,54 @@ __global__ void __launch_bounds__(256) k_ms_pull(uint64_t n, uint32_t k, unsigne
   }
 }
 
+// Several roots, one search (graphs batched as one block-diagonal union: every root in its own
+// component): the roots share source bit 0 of the 64-source word, so the persistent level loop
+// of persist.cu runs the whole search in one cooperative launch.  Levels and per-level counts
+// equal bfs_levels' (the same levels, found in the same order of levels).
+__global__ void k_ms_seed_roots(const uint32_t* __restrict__ roots, uint32_t k, unsigned long long* __restrict__ seen,
+                                unsigned long long* __restrict__ front, int32_t* __restrict__ levels) {
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < k; j += gridDim.x * blockDim.x) {
+    const uint32_t r = roots[j];
+    seen[r] = 1ull;
+    front[r] = 1ull;
+    levels[r] = 0;
+  }
+}
+
+static int bfs_multiroot_persistent(gre_graph g, const uint32_t* droots, uint32_t nroots, int32_t* level, gre_stats* st) {
+  const uint64_t n = g->n;
+  unsigned long long *seen, *fa, *fb, *acc;
+  uint32_t *flist, *flist2;
+  unsigned char* ctl;
+  GRE_CHECK(ws_array(g, WS_A, n, &seen));
+  GRE_CHECK(ws_array(g, WS_B, n, &fa));
+  GRE_CHECK(ws_array(g, WS_C, n, &fb));
+  GRE_CHECK(ws_array(g, WS_E, n, &acc));
+  GRE_CHECK(ws_array(g, WS_F, n, &flist));
+  GRE_CHECK(ws_array(g, WS_G, n, &flist2));
+  GRE_CHECK(ws_array(g, WS_I, msbfs_ctl_bytes(), &ctl));
+  GRE_CHECK(ensure_bins(g, true));
+  GRE_CUDA(cudaMemsetAsync(level, 0xff, sizeof(int32_t) * n, g->stream));
+  GRE_CUDA(cudaMemsetAsync(seen, 0, sizeof(unsigned long long) * n, g->stream));
+  GRE_CUDA(cudaMemsetAsync(fa, 0, sizeof(unsigned long long) * n, g->stream));
+  GRE_CUDA(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * n, g->stream));
+  k_ms_seed_roots<<<grid_for(nroots, 256), 256, 0, g->stream>>>(droots, nroots, seen, fa, level);
+  GRE_LAUNCH_CHECK();
+  uint32_t nl = 0;
+  uint64_t scanned = 0, bytes = 0;
+  std::vector<unsigned long long> found;
+  GRE_CHECK(msbfs_word_persistent(g, 1ull, seen, fa, fb, acc, flist, flist2, level, ctl,
+                                  (unsigned long long*)(ctl + msbfs_ctl_bytes()) - GRE_MAX_RECORDED_SUPERSTEPS, &nl, &scanned,
+                                  &bytes, &found));
+  for (unsigned long long f : found) stats_record(st, f);
+  if (st) {
+    st->supersteps += nl;  // the empty level is not counted, as bfs_levels
+    st->arcs_traversed += scanned;
+    st->algo_bytes += bytes;
+  }
+  return GRE_SUCCESS;
+}
+
 }  // namespace gre
 
 using namespace gre;
@@ -433,7 +481,8 @@ int gre_bfs_multiroot(gre_graph g, const uint32_t* roots, uint32_t nroots, int32
   GRE_CHECK(ws_array(g, WS_H, nroots ? nroots : 1, &droot));
   RunTimer timer(g);
   if (nroots) GRE_CUDA(cudaMemcpyAsync(droot, hs.data(), sizeof(uint32_t) * nroots, cudaMemcpyHostToDevice, g->stream));
-  GRE_CHECK(bfs_levels(g, droot, nroots, dl, st, true));
+  if (nroots > 1 && msbfs_persistent_available(n)) GRE_CHECK(bfs_multiroot_persistent(g, droot, nroots, dl, st));
+  else GRE_CHECK(bfs_levels(g, droot, nroots, dl, st, true));
   uint64_t e = 0;
   GRE_CHECK(count_reached_edges(g, dl, &e));
   GRE_CHECK(perm_out_end(g, dl, dfinal, 1, 4));

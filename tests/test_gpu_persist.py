@@ -44,3 +44,24 @@ def test_persistent_wait_budget_runs_out_cleanly(monkeypatch):
     monkeypatch.delenv("GRE_GRID_WAIT_MS")
     lv, _ = G.msbfs(g, srcs)  # the same graph, the same context: a normal run
     np.testing.assert_array_equal(lv.reshape(64, n), O.Restatement.from_csr(n, off, col).bfs_many(srcs))
+
+
+def test_batched_graphs_bfs_persistent_equals_host_loop(monkeypatch):
+    """A batch of uneven graphs (one block-diagonal union, one root each): the roots share one
+    source bit of the persistent level loop; levels, per-level counts, supersteps and reached edges
+    equal the host-driven direction-optimising BFS's, and each member's levels the oracle's."""
+    parts = [G.rmat_host(s, 8, 60 + i, True) for i, s in enumerate([12, 9, 14, 11, 13])]
+    gs = [G.Graph.from_csr(n, off, col, dir=G.InOut, symmetric=True) for n, off, col in parts]
+    U, voff = G.Graph.union(gs)
+    roots = [int(G.sample_sources(off, 1, i)[0]) + int(voff[i]) for i, (n, off, col) in enumerate(parts)]
+    monkeypatch.setenv("GRE_PERSIST", "0")
+    host, st_host = G.bfs_multiroot(U, roots)
+    monkeypatch.setenv("GRE_PERSIST", "1")
+    pers, st_pers = G.bfs_multiroot(U, roots)
+    np.testing.assert_array_equal(pers, host)
+    assert st_pers.active == st_host.active and st_pers.supersteps == st_host.supersteps
+    assert st_pers.traversed_edges == st_host.traversed_edges
+    for i, (n, off, col) in enumerate(parts):
+        a, b = int(voff[i]), int(voff[i + 1])
+        ref, _ = O.Restatement.from_csr(n, off, col).bfs(roots[i] - a)
+        np.testing.assert_array_equal(pers[a:b], ref)
