@@ -23,6 +23,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "gre_internal.cuh"
 #include "msbfs.cuh"
@@ -386,7 +387,8 @@ __global__ void __launch_bounds__(256) k_ms_pull(uint64_t n, uint32_t k, unsigne
 // Several roots, one search (graphs batched as one block-diagonal union: every root in its own
 // component): the roots share source bit 0 of the 64-source word, so the persistent level loop
 // of persist.cu runs the whole search in one cooperative launch.  Levels and per-level counts
-// equal bfs_levels' (the same levels, found in the same order of levels).
+// equal bfs_levels' (the same levels, found in the same order of levels).  Used on request only
+// (see gre_bfs_multiroot).
 __global__ void k_ms_seed_roots(const uint32_t* __restrict__ roots, uint32_t k, unsigned long long* __restrict__ seen,
                                 unsigned long long* __restrict__ front, int32_t* __restrict__ levels) {
   for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < k; j += gridDim.x * blockDim.x) {
@@ -481,7 +483,12 @@ int gre_bfs_multiroot(gre_graph g, const uint32_t* roots, uint32_t nroots, int32
   GRE_CHECK(ws_array(g, WS_H, nroots ? nroots : 1, &droot));
   RunTimer timer(g);
   if (nroots) GRE_CUDA(cudaMemcpyAsync(droot, hs.data(), sizeof(uint32_t) * nroots, cudaMemcpyHostToDevice, g->stream));
-  if (nroots > 1 && msbfs_persistent_available(n)) GRE_CHECK(bfs_multiroot_persistent(g, droot, nroots, dl, st));
+  // the persistent form only on request (GRE_PERSIST=1): 32 uneven RMAT graphs (scales 12-18,
+  // 2.65M vertices, 6 levels) took 1.86 ms against 1.13 ms for the host loop, whose few levels
+  // cost less than the persistent loop's 8-byte words per vertex
+  const char* pe = getenv("GRE_PERSIST");
+  if (nroots > 1 && pe && strtoul(pe, nullptr, 10) != 0 && msbfs_persistent_available(n))
+    GRE_CHECK(bfs_multiroot_persistent(g, droot, nroots, dl, st));
   else GRE_CHECK(bfs_levels(g, droot, nroots, dl, st, true));
   uint64_t e = 0;
   GRE_CHECK(count_reached_edges(g, dl, &e));

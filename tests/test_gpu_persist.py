@@ -47,9 +47,10 @@ def test_persistent_wait_budget_runs_out_cleanly(monkeypatch):
 
 
 def test_batched_graphs_bfs_persistent_equals_host_loop(monkeypatch):
-    """A batch of uneven graphs (one block-diagonal union, one root each): the roots share one
-    source bit of the persistent level loop; levels, per-level counts, supersteps and reached edges
-    equal the host-driven direction-optimising BFS's, and each member's levels the oracle's."""
+    """A batch of uneven graphs (one block-diagonal union, one root each) through the persistent
+    level loop (on request: GRE_PERSIST=1), the roots sharing one source bit: levels, per-level
+    counts, supersteps and reached edges equal the host-driven direction-optimising BFS's, and
+    each member's levels the oracle's."""
     parts = [G.rmat_host(s, 8, 60 + i, True) for i, s in enumerate([12, 9, 14, 11, 13])]
     gs = [G.Graph.from_csr(n, off, col, dir=G.InOut, symmetric=True) for n, off, col in parts]
     U, voff = G.Graph.union(gs)
@@ -63,5 +64,5 @@ def test_batched_graphs_bfs_persistent_equals_host_loop(monkeypatch):
     assert st_pers.traversed_edges == st_host.traversed_edges
     for i, (n, off, col) in enumerate(parts):
         a, b = int(voff[i]), int(voff[i + 1])
-        ref, _ = O.Restatement.from_csr(n, off, col).bfs(roots[i] - a)
+        ref = O.Restatement.from_csr(n, off, col).bfs(roots[i] - a)[0]
         np.testing.assert_array_equal(pers[a:b], ref)
