@@ -703,7 +703,7 @@ __global__ void __launch_bounds__(256) k_far_split(uint64_t nwords, uint32_t* __
   __shared__ uint32_t stage[8][2 * kStage];
   WarpLists<2, kStage> out(stage[threadIdx.x >> 5]);
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  uint32_t dmin = 0xffffffffu, left = 0;
+  uint32_t dmin = 0xffffffffu, nmoved = 0;
   for (uint64_t base = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) & ~31ull; base < nwords; base += stride) {
     const uint64_t wi = base + (threadIdx.x & 31u);
     uint32_t bits = wi < nwords ? infar[wi] : 0u;
@@ -738,15 +738,15 @@ __global__ void __launch_bounds__(256) k_far_split(uint64_t nwords, uint32_t* __
     }
     if (moved) infar[wi] = fbits & ~moved;
     if (set_bucket) inbucket[wi] = bbits | set_bucket;
-    left += __popc(moved);
+    nmoved += __popc(moved);
   }
   out.flush<0>(counters, near);
   out.flush<1>(counters + 4, blist);
   dmin = __reduce_min_sync(0xffffffffu, dmin);
-  left = __reduce_add_sync(0xffffffffu, left);
+  nmoved = __reduce_add_sync(0xffffffffu, nmoved);
   if ((threadIdx.x & 31u) == 0) {
     if (dmin != 0xffffffffu) atomicMin(counters + 3, dmin);
-    if (left) atomicSub(counters + 2, left);
+    if (nmoved) atomicSub(counters + 2, nmoved);
   }
 }
 
