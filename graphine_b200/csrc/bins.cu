@@ -316,7 +316,8 @@ int degree_key(gre_graph g, const uint64_t* off, std::string* key) {
   return GRE_SUCCESS;
 }
 
-// Times `reps` probe supersteps under the current bins; returns the fastest, in ms.
+// Times five probe supersteps under the current bins; returns the fastest of the last four, in ms
+// (candidates 1-2% apart flipped with the fastest of two).
 int probe(gre_graph g, const DegreeBins& B, const uint64_t* off, const uint32_t* col, const double* x, double* y, float* best_ms) {
   double* partial = nullptr;
   GRE_CUDA(cudaMalloc(&partial, sizeof(double) * (B.n_partials + 1)));
@@ -325,7 +326,7 @@ int probe(gre_graph g, const DegreeBins& B, const uint64_t* off, const uint32_t*
   if (e == cudaSuccess) e = cudaEventCreate(&e1);
   int st = e == cudaSuccess ? GRE_SUCCESS : cuda_status(e, "probe events", __FILE__, __LINE__);
   float best = 1e30f;
-  for (int r = 0; r < 3 && !st; ++r) {
+  for (int r = 0; r < 5 && !st; ++r) {
     cudaEventRecord(e0, g->stream);
     st = rows::reduce_rows(B, off, ProbeGather{col, x}, ProbeStore{y}, partial, g->stream);
     cudaEventRecord(e1, g->stream);
@@ -349,12 +350,16 @@ int tune(gre_graph g, DegreeBins& B, const uint64_t* off, const uint32_t* col, b
   if (e == cudaSuccess) e = cudaMemsetAsync(x, 0, sizeof(double) * g->n, g->stream);
   int st = e == cudaSuccess ? GRE_SUCCESS : cuda_status(e, "tuner buffers", __FILE__, __LINE__);
   float best_ms = 1e30f;
-  for (uint32_t lane_arcs : {2u, 4u, 8u}) {
-    for (uint64_t cta_min : {1024ull, 4096ull, 16384ull}) {
+  // RMAT-26, PageRank superstep with a fixed schedule (lane_arcs / cta_min / hub_chunk): 4 / 16384 /
+  // 65536 8.93 ms, 8 / 8192 8.94, 8 / 16384 8.82, 32 / 16384 8.81, 16 / 16384 8.69, 8 / 65536 8.70,
+  // 16 / 65536 / 131072 8.63
+  for (uint32_t lane_arcs : {2u, 4u, 8u, 16u}) {
+    for (uint64_t cta_min : {4096ull, 16384ull, 65536ull}) {
       if (st) break;
       RowSchedule cand;
       cand.lane_arcs = lane_arcs;
       cand.cta_min = cta_min;
+      cand.hub_chunk = cta_min > 32768 ? 2 * cta_min : 65536;
       float ms = 0;
       st = build_bins(g, B, off, col, cand);
       if (!st) st = probe(g, B, off, col, x, y, &ms);
