@@ -276,6 +276,7 @@ void destroy_graph(gre_graph g) {
   cudaFree(g->rw64);
   free_bins(g->bins_in);
   free_bins(g->bins_out);
+  free_bins(g->bins_sssp);
   cudaFree(g->bc_chunks.rows);
   cudaFree(g->bc_chunks.chunk_row);
   cudaFree(g->bc_chunks.chunk_begin);
@@ -415,6 +416,7 @@ static void drop_derived(gre_graph g) {
   g->indeg = g->outdeg = nullptr;
   free_bins(g->bins_in);
   free_bins(g->bins_out);
+  free_bins(g->bins_sssp);
   cudaFree(g->bc_chunks.rows);
   cudaFree(g->bc_chunks.chunk_row);
   cudaFree(g->bc_chunks.chunk_begin);

@@ -160,6 +160,9 @@ struct gre_graph_s {
   uint64_t max_outdeg = 0, max_indeg = 0;
   gre::Workspace ws;
   gre::DegreeBins bins_in, bins_out;
+  // SSSP's binned passes, when the tuned schedule gives rows more than 8 arcs per lane or a warp
+  // above 16384 arcs (sssp_bins): the pushes are latency-bound and want short chains per lane
+  gre::DegreeBins bins_sssp;
   // Degree-ordered relabelling (GRE_GRAPH_REORDER / gre_graph_reorder): every internal array
   // uses internal ids; perm[i] is the caller's id of internal vertex i (the reference's
   // lvid2vid, DistributedGraph.hpp:57-59) and iperm its inverse.  Null when not relabelled.
@@ -383,6 +386,9 @@ int sssp_split_rows(cudaStream_t stream, uint64_t rows, const uint64_t* off, con
                     uint32_t* ocol, uint32_t* ow, uint64_t* lend);
 // Frontiers of at least n / sssp_binned_divisor() vertices go through the degree bins (0: never);
 // whether heavy passes may pull (GRE_SSSP_BINNED, GRE_SSSP_PULL).
+// The bins SSSP's binned passes use (sssp.cu): the graph's CSR (in = false) or CSC bins, or a copy
+// with at most 8 arcs per lane and a CTA from 16384 arcs when the tuned schedule is wider.
+int sssp_bins(gre_graph g, bool in, const DegreeBins** out);
 uint64_t sssp_binned_divisor();
 bool sssp_pull_enabled();
 // A heavy pass with at least m / sssp_pull_arcs_divisor() arcs pulls whatever its member count

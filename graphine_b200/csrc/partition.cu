@@ -1007,7 +1007,9 @@ int gre_part_sssp(gre_part p, uint32_t src, uint32_t* dist, gre_exchange_fn xchg
   const uint64_t* lend = delta ? p->sp_lend : s->off + 1;  // end of each row's light arcs
   const uint32_t* col = delta ? p->sp_col : s->col;
   const uint32_t* w = delta ? p->sp_w : p->w32;
-  const DegreeBins& B = s->roff == s->off ? s->bins_in : s->bins_out;
+  const DegreeBins* pB = nullptr;  // the part's rows binned as the one-GPU SSSP bins them
+  GRE_CHECK(sssp_bins(s, s->roff == s->off, &pB));
+  const DegreeBins& B = *pB;
   uint32_t *dl, *dist_all, *queue, *pend, *inb, *inb_all, *cand, *recv, *dout;
   uint64_t *deg, *prefix;
   SsspCounters *c, *call;

@@ -830,6 +830,29 @@ static uint64_t pull_arcs_divisor() {
 }
 uint64_t sssp_pull_arcs_divisor() { return pull_arcs_divisor(); }
 
+// The tuner picks the row schedule for the PageRank gather (RMAT-26: 16 arcs per lane, a warp up
+// to 65536 arcs); SSSP's pushes wait on two dependent loads per four arcs, so longer chains per
+// lane cost them (RMAT-26 SSSP 18.0 -> 19.4 ms under that schedule).  Their bins keep at most 8
+// arcs per lane and a CTA from 16384 arcs.
+int sssp_bins(gre_graph g, bool in, const DegreeBins** out) {
+  GRE_CHECK(ensure_bins(g, in));
+  const DegreeBins& B = in ? g->bins_in : g->bins_out;
+  if (B.sched.lane_arcs <= 8 && B.sched.cta_min <= 16384) {
+    *out = &B;
+    return GRE_SUCCESS;
+  }
+  RowSchedule s = B.sched;
+  s.lane_arcs = std::min<uint32_t>(s.lane_arcs, 8);
+  s.cta_min = std::min<uint64_t>(s.cta_min, 16384);
+  s.hub_chunk = 65536;
+  s.seg_window = 0;
+  DegreeBins& S = g->bins_sssp;
+  if (!S.ready || S.sched.lane_arcs != s.lane_arcs || S.sched.cta_min != s.cta_min || S.sched.hub_chunk != s.hub_chunk)
+    GRE_CHECK(build_bins(g, S, in ? g->roff : g->off, in ? g->rcol : g->col, s));
+  *out = &S;
+  return GRE_SUCCESS;
+}
+
 // The relaxation of one frontier pass: tile starts, then k_sssp_relax over one wave of CTAs.
 int sssp_relax_tiles(cudaStream_t stream, const uint32_t* queue, uint64_t nq, const uint64_t* prefix, uint64_t total,
                      uint32_t* tstart, const uint64_t* base, const uint32_t* col, const uint32_t* w, const uint32_t* srcdist,
@@ -904,8 +927,9 @@ static int sssp_one(gre_graph g, uint32_t src, uint32_t* dist, gre_stats* st, bo
   const bool pull = g->w32_symmetric && pull_enabled();
   // large frontiers go through the degree bins of the CSR (the symmetric CSC is the CSR)
   const bool sym = g->symmetric();
-  GRE_CHECK(ensure_bins(g, sym));
-  const DegreeBins& bins = sym ? g->bins_in : g->bins_out;
+  const DegreeBins* pbins = nullptr;
+  GRE_CHECK(sssp_bins(g, sym, &pbins));
+  const DegreeBins& bins = *pbins;
   const uint64_t bdiv = binned_frontier();
   const uint64_t pdiv = pull_arcs_divisor();
   size_t cubbytes = 0;
