@@ -67,12 +67,29 @@ int num_sms() {
   return sms > 0 ? sms : 148;
 }
 
+// The graph's stream is non-blocking: without a wait it would not be ordered after the caller's
+// work on the legacy default stream (PyTorch's default stream; kernels and copies issued without
+// a stream), and could read a device input before that work wrote it, or write a device output
+// that work still reads.  Every call therefore starts by making the graph's stream wait for the
+// legacy stream's work issued so far (an event, no host synchronisation).  Skipped while a stream
+// capture is in progress (the legacy stream cannot be used then): a caller that captures, or that
+// works on streams of its own, orders its buffers itself.
 int use_graph(gre_graph g) {
   if (!g) {
     set_error("null graph handle");
     return GRE_NULL;
   }
   GRE_CUDA(cudaSetDevice(g->device));
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(g->stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+    cudaGetLastError();
+    return GRE_SUCCESS;
+  }
+  if (cudaEventRecord(g->ev_caller, cudaStreamLegacy) != cudaSuccess) {  // another stream is being captured
+    cudaGetLastError();
+    return GRE_SUCCESS;
+  }
+  GRE_CUDA(cudaStreamWaitEvent(g->stream, g->ev_caller, 0));
   return GRE_SUCCESS;
 }
 
@@ -249,6 +266,7 @@ int new_graph(int device, uint32_t flags, gre_graph* out) {
   cudaError_t e1 = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
   cudaError_t e2 = cudaEventCreate(&g->ev0);
   cudaError_t e3 = cudaEventCreate(&g->ev1);
+  if (e3 == cudaSuccess) e3 = cudaEventCreateWithFlags(&g->ev_caller, cudaEventDisableTiming);
   if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
     delete g;
     return cuda_status(e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3), "stream/event create", __FILE__, __LINE__);
@@ -289,6 +307,7 @@ void destroy_graph(gre_graph g) {
   g->ws.release();
   if (g->ev0) cudaEventDestroy(g->ev0);
   if (g->ev1) cudaEventDestroy(g->ev1);
+  if (g->ev_caller) cudaEventDestroy(g->ev_caller);
   if (g->stream) cudaStreamDestroy(g->stream);
   delete g;
 }

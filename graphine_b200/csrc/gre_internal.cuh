@@ -176,6 +176,7 @@ struct gre_graph_s {
   uint64_t* bc_fpool = nullptr;    // per-level frontier words of the batched betweenness
   uint64_t bc_fpool_levels = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev_caller = nullptr;  // orders the stream after the caller's legacy-stream work (use_graph)
   bool symmetric() const { return (flags & GRE_GRAPH_SYMMETRIC) != 0; }
 };
 

@@ -214,6 +214,14 @@ def _ptr(a) -> Optional[int]:
     if hasattr(a, "data_ptr"):  # torch.Tensor
         if not a.is_contiguous():
             raise ValueError("tensors must be contiguous")
+        if getattr(a, "is_cuda", False):
+            import torch
+
+            # the library orders its stream after the legacy default stream (PyTorch's default);
+            # work the caller queued on another stream is finished here
+            cur = torch.cuda.current_stream(a.device)
+            if cur.cuda_stream != 0:
+                cur.synchronize()
         return a.data_ptr()
     raise TypeError(f"unsupported buffer type {type(a)}")
 

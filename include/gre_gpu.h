@@ -17,7 +17,12 @@
  *    device; the library checks which with cudaPointerGetAttributes and copies as needed.
  *    Outputs are caller-allocated.  Host outputs are complete when the call returns.
  *  - One CUDA stream per graph handle.  Calls on one handle are serialised by the caller;
- *    distinct handles may be used from different threads.
+ *    distinct handles may be used from different threads.  Each call first orders the graph's
+ *    stream after the work issued so far on the legacy default stream (where PyTorch's default
+ *    stream and stream-less kernels and copies run), so device buffers written or still read
+ *    there are safe to pass; work on other streams of the caller must be complete (synchronise
+ *    it) before a call that reads or writes its buffers, and during a stream capture the caller
+ *    orders its buffers itself.  Device outputs, like host outputs, are complete on return.
  *  - Symbols under "host utilities" run on the CPU only and need no GPU.
  */
 #ifndef GRE_GPU_H

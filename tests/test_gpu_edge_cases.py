@@ -153,3 +153,34 @@ def test_bc_on_a_long_path(batched):
     np.testing.assert_array_equal(lv, np.arange(n))
     R = O.Restatement.from_csr(n, off, col)  # the reference's engine limit, restated
     assert R.bfs(0)[0].max() == 1024
+
+
+def test_device_inputs_ordered_after_the_default_stream():
+    """A device buffer written on PyTorch's default stream just before the call (behind 0.1 s of
+    queued GPU work) is read only after that write: the library's own stream is non-blocking, and
+    each call orders it after the legacy default stream.  Weights loaded that way give the same
+    distances as the same weights loaded from host memory; a device output that the default
+    stream still reads is not overwritten early either."""
+    import torch
+
+    n, off, col = G.rmat_host(12, 16, 5, True)
+    w_host = np.random.default_rng(1).integers(1, 256, size=len(col), dtype=np.uint32)
+    ref_g = G.Graph.from_csr(n, off, col, dir=G.InOut, symmetric=True)
+    ref_g.loadEdgeProperty(w_host)
+    roots = G.sample_sources(off, 2, 3)
+    ref, _ = G.sssp(ref_g, roots)
+    g = G.Graph.from_csr(n, off, col, dir=G.InOut, symmetric=True)
+    staged = torch.from_numpy(w_host.view(np.int32)).cuda()
+    torch.cuda.synchronize()
+    torch.cuda._sleep(200_000_000)  # about 0.1 s of GPU time, then the copy the call must wait for
+    w = staged.clone()
+    g.loadEdgeProperty(w)
+    got, _ = G.sssp(g, roots)
+    np.testing.assert_array_equal(got, ref)
+    out = torch.zeros(len(roots) * n, dtype=torch.int32, device="cuda")
+    torch.cuda._sleep(200_000_000)
+    before = out.clone()  # reads the zeros after the sleep: the call's writes must come later
+    G.sssp(g, roots, out=out)
+    torch.cuda.synchronize()
+    assert int(before.abs().sum()) == 0
+    np.testing.assert_array_equal(out.cpu().numpy().view(np.uint32), ref.reshape(-1))
