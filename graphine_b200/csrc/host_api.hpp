@@ -19,5 +19,8 @@ int host_write_roots(const char* prefix, const uint32_t* roots, uint32_t count);
 int host_read_roots(const char* prefix, std::vector<uint32_t>* roots);
 void host_build_csr(uint64_t n, const std::vector<uint32_t>& src, const std::vector<uint32_t>& dst,
                     bool by_dst, std::vector<uint64_t>* off, std::vector<uint32_t>* col);
+// the per-thread error text of the C ABI (graph.cu)
+void set_error(const char* fmt, ...);
+void clear_error();
 
 }  // namespace gre

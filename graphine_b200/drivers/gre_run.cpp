@@ -138,11 +138,23 @@ int main(int argc, char** argv) {
   if (argc < 3) {
     fprintf(stderr, "usage: %s pagerank|pagerank_iter|pagerank_delta|bfs|sssp|sssp1|cc|cin|bc prefix [ascii] "
                     "[edgelists|partition [nparts]]\n"
-                    "       %s part_bfs|part_sssp|part_cc|part_pagerank|part_pagerank_iter prefix --ranks P --rank r --id-file F [--device d]\n",
-            argv[0], argv[0]);
+                    "       %s part_bfs|part_sssp|part_cc|part_pagerank|part_pagerank_iter prefix --ranks P --rank r --id-file F [--device d]\n"
+                    "       %s graphpar prefix nparts\n",
+            argv[0], argv[0], argv[0]);
     return 2;
   }
   const std::string algo(argv[1]), prefix(argv[2]);
+  if (algo == "graphpar") {  // the offline partitioner, as usr/debug/test_graphPar.cpp
+    const uint32_t nparts = argc > 3 ? (uint32_t)strtoul(argv[3], nullptr, 10) : 0u;
+    std::vector<uint64_t> counts(nparts ? nparts : 1);
+    const int st = gre_partition_edges(prefix.c_str(), nparts, counts.data());
+    if (st) {
+      fprintf(stderr, "%s\n", gre_last_error());
+      return st;
+    }
+    for (uint32_t r = 0; r < nparts; ++r) printf("part %u: %llu edges\n", r, (unsigned long long)counts[r]);
+    return 0;
+  }
   if (algo.rfind("part_", 0) == 0) {
     try {
       return run_partitioned(algo, prefix, argc, argv);

@@ -167,6 +167,7 @@ def lib() -> C.CDLL:
             "gre_write_roots": (I32, [C.c_char_p, P, U32]),
             "gre_read_roots": (I32, [C.c_char_p, P, U32, C.POINTER(U32)]),
             "gre_sssp_weight": (U32, [U64, U32, U32]),
+            "gre_partition_edges": (I32, [C.c_char_p, U32, P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -575,6 +576,14 @@ def write_edgelists(prefix: str, n: int, off, col, nfiles: int = 4) -> None:
     o, c = _as(off, np.uint64), _as(col, np.uint32)
     _check(lib().gre_write_edgelists(prefix.encode(), n, len(c), _ptr(o), _ptr(c) if len(c) else None, nfiles),
            "gre_write_edgelists")
+
+
+def partition_edges(prefix: str, nparts: int) -> np.ndarray:
+    """Split <prefix>.edges.<i> into <prefix>.part.<nparts>.<r> (and the .outdegree / .scatterMap
+    files) as the reference's offline partitioner does; returns the edges per part.  Host only."""
+    counts = np.zeros(nparts, np.uint64)
+    _check(lib().gre_partition_edges(prefix.encode(), nparts, _ptr(counts)), "gre_partition_edges")
+    return counts
 
 
 def write_roots(prefix: str, roots) -> None:

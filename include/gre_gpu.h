@@ -347,6 +347,15 @@ int gre_read_roots(const char* prefix, uint32_t* roots, uint32_t capacity, uint3
 int gre_part_layout(uint64_t n, uint32_t nparts, uint64_t* slots, uint32_t* index);
 /* The SSSP weight function of gre_graph_set_weights_hash. */
 uint32_t gre_sssp_weight(uint64_t wseed, uint32_t u, uint32_t v);
+/* Offline edge partitioner: the reference's single-process EdgePartition::divideEdges
+ * (include/Graph/GraphIngress.hpp:1272-1452, usr/debug/test_graphPar.cpp).  Reads <prefix>.meta
+ * and the edge lists <prefix>.edges.<i>, places every edge on one of nparts parts by the
+ * reference's greedy vertex-cut rule (balance + parts already holding its ends; ties by
+ * (u + v) mod ties), and writes <prefix>.part.<nparts>.<r> (the edges as uint64 pairs: what an
+ * np = nparts run and gre_graph_load_parts load), <prefix>.outdegree.<nparts>.<p> and
+ * <prefix>.scatterMap.<nparts>.<p>.  part_edges (nparts entries, may be NULL) receives the edge
+ * count of each part.  nparts in 1..64.  Files are written afresh. */
+int gre_partition_edges(const char* prefix, uint32_t nparts, uint64_t* part_edges);
 
 #ifdef __cplusplus
 }

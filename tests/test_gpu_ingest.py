@@ -165,3 +165,27 @@ def test_saved_partitions_errors():
         with pytest.raises(G.GreError) as e:
             G.Graph.load_parts(p, 0)
         assert e.value.status == G.GRE_INVALID_ARG
+
+
+@pytest.mark.parametrize("P", [2, 3])
+def test_partitioner_output_loads_as_the_graph(P):
+    """Edge lists split by gre_partition_edges (the reference's offline partitioner) load back
+    through gre_graph_load_parts as the same graph: the merged CSR holds the parts' edges in rank
+    order, and BFS / CC on it equal the oracle's on the original edge lists."""
+    n, off, col = G.rmat_host(11, 8, 9, True)
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "g")
+        G.write_edgelists(p, n, off, col, 4)
+        counts = G.partition_edges(p, P)
+        assert int(counts.sum()) == len(col) and (counts > 0).all()
+        parts = [np.fromfile(p + f".part.{P}.{r}", dtype=np.uint64).reshape(-1, 2) for r in range(P)]
+        g = G.Graph.load_parts(p, P, G.InOut, symmetric=True)
+    allp = np.concatenate(parts).astype(np.int64)
+    order = np.argsort(allp[:, 0], kind="stable")
+    o2, c2 = g.csr()
+    np.testing.assert_array_equal(o2, off)
+    np.testing.assert_array_equal(c2, allp[order, 1].astype(np.uint32))
+    R = O.Restatement.from_csr(n, off, col)
+    roots = G.sample_sources(off, 2, 1)
+    np.testing.assert_array_equal(G.bfs(g, roots)[0].reshape(2, n), R.bfs_many(roots))
+    np.testing.assert_array_equal(G.cc(g)[0], R.cc()[0])
