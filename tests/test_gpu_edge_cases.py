@@ -170,6 +170,8 @@ def test_device_inputs_ordered_after_the_default_stream():
     roots = G.sample_sources(off, 2, 3)
     ref, _ = G.sssp(ref_g, roots)
     g = G.Graph.from_csr(n, off, col, dir=G.InOut, symmetric=True)
+    g.loadEdgeProperty(np.ones(len(col), np.uint32))  # the weight array exists: no allocation orders the load below
+    G.sssp(g, roots)  # and the run's scratch too
     staged = torch.from_numpy(w_host.view(np.int32)).cuda()
     torch.cuda.synchronize()
     torch.cuda._sleep(200_000_000)  # about 0.1 s of GPU time, then the copy the call must wait for
