@@ -205,6 +205,23 @@ class SynchronousEngine {
   gre_stats st_{};
 };
 
+// Graph::EdgePartition (Graph/GraphIngress.hpp:1272-1452): the offline partitioner, driven as
+// usr/debug/test_graphPar.cpp drives it (`EdgePartition par; par.divideEdges(prefix, n);`).  It
+// writes <prefix>.part.<n>.<r>, .outdegree.<n>.<p> and .scatterMap.<n>.<p> from the edge lists,
+// on the host (gre_partition_edges); errors throw gre::Error instead of printing.
+class EdgePartition {
+ public:
+  void divideEdges(const std::string& prefix, const int n) {
+    counts_.assign(n > 0 ? n : 1, 0);
+    check(gre_partition_edges(prefix.c_str(), n > 0 ? (uint32_t)n : 0u, counts_.data()), "gre_partition_edges");
+    counts_.resize(n > 0 ? n : 0);
+  }
+  const std::vector<uint64_t>& partEdges() const { return counts_; }  // edges per part of the last split
+
+ private:
+  std::vector<uint64_t> counts_;
+};
+
 // COMM::Underlying (Comm/CommUnderlying.hpp:25-80) of an np > 1 job: the library's NCCL
 // communicator over the job's ranks, rank() and size() as in the reference.  Agreeing on the
 // ranks (MPI_Init's part) is the job's: rank 0 makes the id with uniqueId() and hands it to every

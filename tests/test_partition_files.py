@@ -90,3 +90,35 @@ def test_partition_edges_errors(tmp_path):
     with pytest.raises(G.GreError) as e:
         G.partition_edges(str(tmp_path / "g"), 2)
     assert e.value.status == G.GRE_INVALID_ARG
+
+
+def test_cpp_mirror_drives_the_partitioner(tmp_path):
+    """A driver written as usr/debug/test_graphPar.cpp (EdgePartition par; par.divideEdges(prefix,
+    n)) compiles against the C++ mirror include/gre/gre.hpp and writes the same parts as
+    gre_partition_edges."""
+    import shutil
+
+    if not shutil.which("g++"):
+        pytest.skip("no host C++ compiler")
+    src = tmp_path / "graphpar.cpp"
+    src.write_text(
+        '#include "gre/gre.hpp"\n#include <cstdlib>\n'
+        "int main(int argc, char** argv) {\n"
+        "  gre::EdgePartition par;\n"
+        "  par.divideEdges(argv[1], atoi(argv[2]));\n"
+        "  return 0;\n}\n")
+    exe = tmp_path / "graphpar"
+    libdir = os.path.join(ROOT, "graphine_b200")
+    subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include", str(src),
+                    "-L", libdir, "-lgre_gpu", f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True, capture_output=True,
+                   timeout=300)
+    n, off, col = G.rmat_host(9, 8, 11, True)
+    a, b = tmp_path / "a", tmp_path / "b"
+    a.mkdir()
+    b.mkdir()
+    for d in (a, b):
+        G.write_edgelists(str(d / "g"), n, off, col, 3)
+    subprocess.run([str(exe), str(a / "g"), "4"], check=True, capture_output=True, timeout=300)
+    G.partition_edges(str(b / "g"), 4)
+    for r in range(4):
+        assert (a / f"g.part.4.{r}").read_bytes() == (b / f"g.part.4.{r}").read_bytes()
